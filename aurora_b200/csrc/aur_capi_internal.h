@@ -1,0 +1,82 @@
+// aur_capi_internal.h — handle layouts and helpers shared by the C-ABI sources.
+#pragma once
+#include "aurora_b200.h"
+#include "aur_kernels.h"
+#include <string>
+#include <vector>
+
+struct aur_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    float* kelemen = nullptr;                  // 21 tables x 2048 floats
+    bool kel_ready[aur::kAlbedoRefl] = {};
+    unsigned long long* counters = nullptr;    // 8 render counters
+};
+
+struct aur_bvh {
+    aur_ctx* ctx = nullptr;
+    aur::DeviceBvh bvh;
+    int* tri_attr = nullptr;                   // device, per original triangle id
+    bool owns_attr = false;
+    bool owned_by_scene = false;
+};
+
+struct aur_scene {
+    aur_ctx* ctx = nullptr;
+    aur_bvh bvh;                               // owned_by_scene = true
+    // device buffers
+    float* corner_n = nullptr;
+    float* corner_uv = nullptr;
+    aur::Attr* attrs = nullptr;
+    aur::Material* mats = nullptr;
+    aur::Light* lights = nullptr;
+    aur::Texture* texs = nullptr;
+    float* texels = nullptr;
+    // host copies
+    std::vector<aur::Material> h_mats;
+    std::vector<aur::Light> h_lights;
+    std::vector<aur::Texture> h_texs;
+    uint32_t ntri = 0, nattr = 0, ntexel_floats = 0;
+    aur::Camera cam{};
+    aur::DevScene dev() const;
+};
+
+namespace aur {
+
+aur_status fail(aur_status s, const std::string& msg);
+aur_status cuda_fail(cudaError_t e, const char* where);
+bool is_device_ptr(const void* p);
+cudaError_t ctx_kelemen_ensure(aur_ctx* ctx, int refl_index);
+int kelemen_index(float reflectance);
+aur_status bvh_options(const aur_bvh_opts* o, BvhBuildOptions* out);
+aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathParams* p);
+aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film, aur_render_stats* stats);
+
+struct DeviceGuard {
+    explicit DeviceGuard(int dev);
+    ~DeviceGuard();
+    int prev_ = 0;
+};
+
+struct DevIn {
+    const void* ptr = nullptr;
+    void* owned = nullptr;
+    cudaStream_t stream = nullptr;
+    cudaError_t init(const void* p, size_t bytes, size_t align, cudaStream_t s);
+    ~DevIn();
+};
+
+struct DevOut {
+    void* ptr = nullptr;
+    void* owned = nullptr;
+    void* user = nullptr;
+    size_t size = 0;
+    bool host = false;
+    cudaStream_t stream = nullptr;
+    cudaError_t init(void* p, size_t bytes, size_t align, cudaStream_t s);
+    cudaError_t finish();
+    ~DevOut();
+};
+
+}  // namespace aur

@@ -1,0 +1,148 @@
+// aur_integrator.cuh — the per-path MIS loop of Integrator::integrateCameraSample
+// (Aurora/src/frontend/integrator.cpp:152-300) for one camera path, as a
+// device function shared by the plain megakernel and the tests' probes.
+//
+// Faithful to the reference: emission only on camera rays; one light chosen
+// uniformly among the "visible" ones and the result scaled by their count
+// (integrator.cpp:100-130); Lambert vertices use light sampling only
+// (integrateDirectLight :33-54), specular vertices the power-heuristic MIS of
+// integrateDirectMIS (:56-98); throughput f*cos/pdf; a cumulative continue
+// probability and roulette when bounces > mindepth (:219-248); firefly clamp
+// (:278-281). The reference traces one more closest-hit ray after the last
+// shaded vertex whose hit is never shaded (it only matters for environment
+// lights, which are out of scope); that ray is skipped here.
+#pragma once
+#include "aur_traverse.cuh"
+
+namespace aur {
+
+struct DevScene {
+    const BvhNode* nodes;
+    const BvhTri* tris;
+    ShadeScene sh;
+    Camera cam;
+};
+
+struct PathParams {
+    int max_depth, min_depth;
+    int spp, sample_offset;
+    uint32_t seed;
+};
+
+struct RayCounts { uint32_t closest = 0, shadow = 0; TraceWork work; };
+
+// Picks the k-th light for which light_visible() holds; returns -1 if none.
+__device__ __forceinline__ int pick_visible_light(const ShadeScene& sh, float3 P, float3 N, float u, int* nvis) {
+    int n = 0;
+    for (int i = 0; i < sh.nlights; ++i) n += light_visible(sh.lights[i], P, N) ? 1 : 0;
+    *nvis = n;
+    if (n == 0) return -1;
+    int k = (int)(u * (float)n);
+    k = k < n ? k : n - 1;
+    for (int i = 0; i < sh.nlights; ++i) {
+        if (light_visible(sh.lights[i], P, N)) {
+            if (k == 0) return i;
+            --k;
+        }
+    }
+    return -1;
+}
+
+// integrateDirect (integrator.cpp:100-130) with integrateDirectLight / integrateDirectMIS.
+__device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Frame& f, const Brdf& brdf,
+                                                   const PathRng& rng, int vtx, RayCounts& rc) {
+    float3 res = mk(0.f, 0.f, 0.f);
+    if (brdf.lobe != LOBE_MATTE && brdf.lobe != LOBE_SPEC) return res;
+    int nvis;
+    const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
+    if (li < 0) return res;
+    const Light L = sc.sh.lights[li];
+    const LightSample ls = light_sample(L, f.P, rng.u(vertex_dim(vtx, kDimLightSample)),
+                                        rng.u(vertex_dim(vtx, kDimLightSample + 1)));
+    float cost = dot(f.N, ls.dir);
+    if (brdf.lobe == LOBE_MATTE) {
+        if (cost >= 0.f && ls.pdf > 0.f) {
+            ++rc.shadow;
+            if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.work))
+                res += cdiv((ls.color * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
+        }
+    } else {
+        if (cost > 0.f && ls.pdf > 0.f) {
+            const float bp = brdf_pdf(brdf, ls.dir, f.V, f.N);
+            if (bp > 0.f) {
+                ++rc.shadow;
+                if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.work)) {
+                    const float w = power_heuristic(ls.pdf, bp);
+                    res += cdiv(((ls.color * w) * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
+                }
+            }
+        }
+        const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimMisBrdf)),
+                                          rng.u(vertex_dim(vtx, kDimMisBrdf + 1)));
+        cost = dot(f.N, bs.dir);
+        if (cost > 0.f) {
+            float maxt = bs.maxt;
+            const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
+            if (lp > 0.f && bs.pdf > 0.f) {
+                ++rc.shadow;
+                if (!bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.work)) {
+                    const float w = power_heuristic(bs.pdf, lp);
+                    res += cdiv(((bs.color * w) * L.le) * cost, bs.pdf);
+                }
+            }
+        }
+    }
+    return res * (float)nvis;
+}
+
+enum RayKind : int { RAY_CAMERA = 0, RAY_DIFFUSE = 1, RAY_SPECULAR = 2 };
+
+// One camera path; returns the clamped radiance, sets *alpha to 1 on a camera hit.
+__device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathParams& p, int px, int py,
+                                                 const PathRng& rng, RayCounts& rc, float* alpha) {
+    RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+    Hit h;
+    ++rc.closest;
+    *alpha = 0.f;
+    float3 Lo = mk(0.f, 0.f, 0.f);
+    if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) return Lo;
+    *alpha = 1.f;
+    float3 T = mk(1.f, 1.f, 1.f);
+    float cont = 1.f;
+    bool matte_path = false;
+    int kind = RAY_CAMERA;
+    int bounces = 0;
+    for (int vtx = 0; vtx < p.max_depth; ++vtx) {
+        const Frame f = hit_frame(sc.sh, h.prim, h.t, h.u, h.v, ray.o, ray.d, true);
+        const Attr at = sc.sh.attrs[f.attr];
+        if (kind == RAY_DIFFUSE) matte_path = true;
+        if (kind == RAY_CAMERA) Lo += T * at.emission;
+        const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte_path,
+                                   rng.u(vertex_dim(vtx, kDimLobe)));
+        Lo += integrate_direct(sc, f, brdf, rng, vtx, rc) * T;
+        const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
+                                          rng.u(vertex_dim(vtx, kDimBrdf + 1)));
+        if (bs.pdf <= 0.f) break;
+        const float cosl = dot(f.N, bs.dir);
+        T *= cdiv(bs.color * cosl, bs.pdf);
+        if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
+        if (is_black(T)) break;
+        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
+        if (bounces > p.min_depth) {
+            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
+            T = cdiv(T, cont);
+        }
+        ++bounces;
+        if (vtx + 1 >= p.max_depth) break;   // the reference's unshaded last ray
+        ray.o = f.P;
+        ray.d = bs.dir;
+        ray.mint = kRayBias;
+        ray.maxt = bs.maxt;
+        ++rc.closest;
+        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) break;
+    }
+    while (Lo.x > kFirefly || Lo.y > kFirefly || Lo.z > kFirefly) Lo *= 0.2f;
+    return Lo;
+}
+
+}  // namespace aur

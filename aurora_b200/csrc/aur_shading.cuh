@@ -1,0 +1,426 @@
+// aur_shading.cuh — scene records and the per-vertex shading math of the
+// Aurora path loop: camera rays, Lambert / Cook-Torrance(Beckmann) / Kelemen /
+// metal lobes, square and sphere area lights, texture lookups and the exact
+// FP32 Moller-Trumbore triangle test. Every function is __host__ __device__
+// and stateless; random numbers are passed in by the caller.
+//
+// Reference semantics restated here (file:line in espennordahl/Aurora):
+//   camera ray                Aurora/src/frontend/camera.cpp:34-62
+//   Lambert                   Aurora/src/shading/bxdfs/lambert.h:44-80
+//   Cook-Torrance (Beckmann)  Aurora/src/shading/bxdfs/cookTorrance.cpp:40-144
+//   Kelemen lobe choice       Aurora/src/shading/materials/kelemenMaterial.cpp:180-255
+//   metal lobe choice         Aurora/src/shading/materials/metalMaterial.cpp:32-62
+//   matte / constant          matteMaterial.cpp:30-35, constantMaterial.cpp:19-24, bxdfs/constant.cpp:23-37
+//   square light              Aurora/src/lights/squareLight.h:57-122, squareLight.cpp:20-52
+//   triangle test             Aurora/src/geometry/renderableTriangle.cpp:33-123
+//   texture2D (nearest)       Aurora/src/shading/shaders/texture2DShader.h:28-31, frontend/texture2D.cpp:48-72
+// The sphere light has no reference counterpart (uniform cone sampling of the
+// subtended solid angle, as in Shirley & Wang 1994 / pbrt v3 section 14.2).
+#pragma once
+#include "aur_core.cuh"
+
+namespace aur {
+
+// ------------------------------------------------------------------ records
+enum MatType : int { MAT_MATTE = 0, MAT_KELEMEN = 1, MAT_COOKTORRANCE = 2, MAT_METAL = 3, MAT_CONSTANT = 4 };
+enum LobeType : int { LOBE_MATTE = 0, LOBE_SPEC = 1, LOBE_MIRROR = 2, LOBE_CONSTANT = 3 };  // brdf.h BrdfType
+enum LightType : int { LIGHT_SQUARE = 0, LIGHT_SPHERE = 1 };
+
+struct Material {            // 80 B
+    int type;
+    int diff_tex, spec_tex, rough_tex;   // texture index or -1
+    float3 diff;             // matte colour / Kelemen diffusecolor
+    float3 spec;             // Kelemen speccolor / CT colour / metal reflectance
+    float3 gain;             // metal gain
+    float rough, rough_b;    // roughness (metal: roughnessA, roughnessB)
+    float refl;              // Kelemen reflectance (selects the albedo table)
+    float mix;               // metal mix
+    int table;               // Kelemen albedo table index (64x32 floats each)
+    int pad;
+};
+struct Attr {                // AttributeState: material + emission (attributeState.h)
+    int material;
+    float3 emission;
+};
+struct Light {
+    int type;
+    float xs, ys, radius;
+    float3 p[4];             // square corners in camera space (squareLight.cpp:28-48)
+    float3 n;                // lightN = normalize(cross(p1-p2, p2-p3))
+    float3 le;               // colour * 2^exposure
+    float3 center;           // sphere centre (camera space)
+    float m[16];             // object-to-camera, row major (the square's sample mapping)
+};
+struct Texture { int w, h, offset, pad; };   // texels: RGB float, offset in floats
+struct Camera { float fov; int w, h; int pad; };
+
+struct ShadeScene {          // device pointers for the shading stage
+    const Material* mats;
+    const Attr* attrs;
+    const Light* lights;
+    const Texture* texs;
+    const float* texels;
+    const float* albedo;     // Kelemen tables, [table][cos 64][rough 32]
+    const float* corner_n;   // per-corner normals, 9 floats per triangle
+    const float* corner_uv;  // per-corner uvs, 6 floats per triangle
+    const int* tri_attr;     // attribute index per triangle
+    int nlights;
+};
+
+struct RayF { float3 o; float mint; float3 d; float maxt; };
+
+// ------------------------------------------------------------------ camera
+AUR_HD RayF camera_ray(const Camera& cam, int px, int py, float j1, float j2) {
+    float fovx = cam.fov;
+    float fovy = ((float)cam.h / (float)cam.w) * fovx;
+    float u = (float)px + j1;
+    float v = (float)py + j2;
+    float3 d = mk(((2.f * u - (float)cam.w) / (float)cam.w) * fovx,
+                  ((-2.f * v + (float)cam.h) / (float)cam.h) * fovy, -1.f);
+    RayF r;
+    r.d = normalize(d);
+    r.o = mk(0.f, 0.f, 0.f);
+    r.mint = 0.1f;
+    r.maxt = 10000000.f;
+    return r;
+}
+
+// ------------------------------------------------------------------ triangle
+// Exact restatement of RenderableTriangle::intersect (renderableTriangle.cpp:68-98).
+// The __f*_rn intrinsics forbid FMA contraction on the device, and the host
+// build uses -ffp-contract=off, so both sides round every operation the same
+// way. IEEE reciprocal (__frcp_rn) equals the reference's 1.f/divisor.
+#ifdef __CUDA_ARCH__
+#define AUR_MUL(a, b) __fmul_rn(a, b)
+#define AUR_ADD(a, b) __fadd_rn(a, b)
+#define AUR_SUB(a, b) __fsub_rn(a, b)
+#define AUR_RCP(a) __frcp_rn(a)
+#else
+#define AUR_MUL(a, b) ((a) * (b))
+#define AUR_ADD(a, b) ((a) + (b))
+#define AUR_SUB(a, b) ((a) - (b))
+#define AUR_RCP(a) (1.f / (a))
+#endif
+AUR_HD float xdot(float3 a, float3 b) { return AUR_ADD(AUR_ADD(AUR_MUL(a.x, b.x), AUR_MUL(a.y, b.y)), AUR_MUL(a.z, b.z)); }
+AUR_HD float3 xcross(float3 a, float3 b) {
+    return mk(AUR_SUB(AUR_MUL(a.y, b.z), AUR_MUL(a.z, b.y)),
+              AUR_SUB(AUR_MUL(a.z, b.x), AUR_MUL(a.x, b.z)),
+              AUR_SUB(AUR_MUL(a.x, b.y), AUR_MUL(a.y, b.x)));
+}
+AUR_HD float3 xsub(float3 a, float3 b) { return mk(AUR_SUB(a.x, b.x), AUR_SUB(a.y, b.y), AUR_SUB(a.z, b.z)); }
+// Returns true and writes t, b1 (weight of vertex 1 = u), b2 (vertex 2 = v) on a hit in [mint, maxt].
+AUR_HD bool tri_intersect(float3 p1, float3 e1, float3 e2, float3 o, float3 d, float mint, float maxt,
+                          float* t_out, float* b1_out, float* b2_out) {
+    float3 s1 = xcross(d, e2);
+    float divisor = xdot(s1, e1);
+    if (divisor == 0.f) return false;
+    float inv = AUR_RCP(divisor);
+    float3 dd = xsub(o, p1);
+    float b1 = AUR_MUL(xdot(dd, s1), inv);
+    if (b1 < 0.f || b1 > 1.f) return false;
+    float3 s2 = xcross(dd, e1);
+    float b2 = AUR_MUL(xdot(d, s2), inv);
+    if (b2 < 0.f || AUR_ADD(b1, b2) > 1.f) return false;
+    float t = AUR_MUL(xdot(e2, s2), inv);
+    if (t < mint || t > maxt) return false;
+    *t_out = t; *b1_out = b1; *b2_out = b2;
+    return true;
+}
+
+// ------------------------------------------------------------------ textures
+AUR_HD int aur_floor(float x) { return (int)x - (x < 0.f && (float)(int)x != x); }   // math_utils.h floor
+AUR_HD float3 tex_read(const ShadeScene& s, int tex, float su, float sv) {
+    Texture t = s.texs[tex];
+    float fs = su - (float)aur_floor(su);
+    float ft = 1.f - (sv - (float)aur_floor(sv));
+    int x = aur_floor(fs * (float)t.w);
+    int y = aur_floor(ft * (float)t.h);
+    if (y == t.h) y -= 1;
+    if (x == t.w) x -= 1;
+    x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
+    y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
+    const float* p = s.texels + t.offset + 3 * (y * t.w + x);
+    return mk(p[0], p[1], p[2]);
+}
+
+// ------------------------------------------------------------------ BRDF lobes
+struct Brdf {                // an instantiated lobe: BrdfState{Brdf*, bxdfParameters*}
+    int lobe;                // LobeType
+    float3 color;            // Lambert albedo or CT colour
+    float rough;             // CT roughness
+};
+struct BrdfSample { float3 dir; float pdf; float3 color; float maxt; };
+
+AUR_HD float ct_d(float rough, float cosa, float tana) {        // cookTorrance.cpp:40-45
+    float rough2 = fmaxf(0.001f, rough * rough);
+    float e = expf(-(tana * tana) / rough2);
+    float div = rough2 * kPi * powf(cosa, 3.f);
+    return e / div;
+}
+
+AUR_HD BrdfSample brdf_sample(const Brdf& b, float3 V, float3 N, float r1, float r2) {
+    BrdfSample s;
+    if (b.lobe == LOBE_MATTE) {                                      // lambert.h:44-62
+        float3 dir = sample_hemisphere_uniform(r1, r2);
+        s.dir = normalize(tangent_to_world(dir, N));
+        s.pdf = kInvPi * 0.5f;
+        s.color = b.color * kInvPi;
+        s.maxt = 1000000.f;
+        return s;
+    }
+    if (b.lobe == LOBE_SPEC) {                                       // cookTorrance.cpp:47-99
+        float z = cosf(atanf(b.rough * sqrtf(-logf(1.f - r1))));
+        float r = sqrtf(fmaxf(0.f, 1.f - z * z));
+        float phi = kPi * 2.f * r2;
+        float3 dir = normalize(mk(r * cosf(phi), r * sinf(phi), z));
+        float3 H = normalize(tangent_to_world(dir, N));
+        float vdoth = dot(V, H);
+        float3 L = normalize((H * 2.f) * vdoth - V);
+        float ndoth = dot(N, H);
+        s.color = mk(0.f, 0.f, 0.f);
+        s.pdf = 1.f;
+        if (vdoth > 0.0001f) {
+            float tana = (ndoth > 0.999f) ? 0.f : tanf(acosf(ndoth));
+            float D = ct_d(b.rough, ndoth, tana);
+            D = fminf(D, 1000.f);
+            s.pdf = D / (4.f * vdoth);
+            s.color = b.color * (D / (4.f * vdoth * vdoth));
+            if (s.pdf > 100000.f) { s.pdf *= 0.01f; s.color *= 0.01f; }
+        }
+        s.dir = L;
+        s.maxt = 10000000.f;
+        return s;
+    }
+    // constant (light geometry): Sample3D() -> pdf 0 ends the path (constant.cpp:23-25)
+    s.dir = mk(0.f, 1.f, 0.f); s.pdf = 0.f; s.color = mk(0.f, 0.f, 0.f); s.maxt = 0.f;
+    return s;
+}
+
+AUR_HD float3 brdf_eval(const Brdf& b, float3 L, float3 V, float3 N) {
+    if (b.lobe == LOBE_MATTE) {                                      // lambert.h:68-76
+        return dot(L, N) > 0.f ? b.color * kInvPi : mk(0.f, 0.f, 0.f);
+    }
+    if (b.lobe == LOBE_SPEC) {                                       // cookTorrance.cpp:125-144
+        float3 H = normalize(L + V);
+        float vdoth = dot(V, H), vdotn = dot(V, N), ndoth = dot(H, N), ldotn = dot(L, N);
+        float r2 = b.rough * b.rough;
+        float ta = tanf(acosf(ndoth));
+        float D = (1.f / (r2 * kPi * powf(ndoth, 3.f))) * expf(-(ta * ta) / r2);
+        if (vdoth <= 0.001f || ldotn <= 0.001f || vdotn <= 0.001f || isnan(D)) return mk(0.f, 0.f, 0.f);
+        return b.color * (D / (4.f * vdoth * vdoth));
+    }
+    return mk(0.f, 0.f, 0.f);
+}
+
+AUR_HD float brdf_pdf(const Brdf& b, float3 L, float3 V, float3 N) {
+    if (b.lobe == LOBE_MATTE) return kInvPi * 0.5f;                  // lambert.h:78-80
+    if (b.lobe == LOBE_SPEC) {                                       // cookTorrance.cpp:101-117
+        float3 H = normalize(L + V);
+        float vdoth = dot(V, H), ndoth = dot(N, H);
+        float D = ct_d(b.rough, ndoth, tanf(acosf(ndoth)));
+        if (isnan(D)) D = 0.f;
+        return D / (4.f * vdoth);
+    }
+    return 0.f;
+}
+
+// Kelemen directional-albedo lookup (kelemenMaterial.cpp:180-212). The
+// reference's roughnessB = max(roughnessA+1, 31) is kept (it always reads the
+// last roughness column); the column index is clamped to the table so that
+// roughness 1 stays in bounds (the reference reads past the table there).
+AUR_HD float kelemen_albedo(const float* table, float costheta, float roughness) {
+    int i = aur_floor(costheta * (kAlbedoCos - 1));
+    int ra = aur_floor(roughness * (kAlbedoRough - 1));
+    int rb = ra + 1 > kAlbedoRough - 1 ? ra + 1 : kAlbedoRough - 1;
+    i = i < 0 ? 0 : (i > kAlbedoCos - 1 ? kAlbedoCos - 1 : i);
+    ra = ra < 0 ? 0 : (ra > kAlbedoRough - 1 ? kAlbedoRough - 1 : ra);
+    rb = rb > kAlbedoRough - 1 ? kAlbedoRough - 1 : rb;
+    int i1 = i + 1 < kAlbedoCos - 1 ? i + 1 : kAlbedoCos - 1;
+    float va = table[i * kAlbedoRough + ra];
+    float vb = table[i1 * kAlbedoRough + ra];
+    float mixc = costheta * (kAlbedoCos - 1) - (float)i;
+    float resA = (1.f - mixc) * va + mixc * vb;
+    va = table[i * kAlbedoRough + rb];
+    vb = table[i1 * kAlbedoRough + rb];
+    float resB = (1.f - mixc) * va + mixc * vb;
+    float rmix = roughness * (kAlbedoRough - 1) - (float)ra;
+    return (1.f - rmix) * resA + rmix * resB;
+}
+
+// Material::getBrdf for every supported material. `lobe_u` is the vertex's
+// lobe-choice random number; `st` the interpolated uv.
+AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float su, float sv,
+                     bool matte_path, float lobe_u) {
+    Material m = s.mats[mat_id];
+    Brdf b;
+    if (m.type == MAT_MATTE) {
+        b.lobe = LOBE_MATTE;
+        b.color = m.diff_tex >= 0 ? tex_read(s, m.diff_tex, su, sv) : m.diff;
+        b.rough = 0.f;
+        return b;
+    }
+    if (m.type == MAT_KELEMEN || m.type == MAT_COOKTORRANCE) {
+        float rough = m.rough_tex >= 0 ? tex_read(s, m.rough_tex, su, sv).x : m.rough;
+        if (matte_path) rough = rough * (1.f - kCausticBlur) + kCausticBlur;
+        b.lobe = LOBE_SPEC;
+        b.color = m.spec_tex >= 0 ? tex_read(s, m.spec_tex, su, sv) : m.spec;
+        b.rough = rough;
+        if (m.type == MAT_KELEMEN && m.refl < 1.f) {
+            float c = dot(N, V);
+            c = c < 0.f ? 0.f : (c > 1.f ? 1.f : c);
+            float albedo = kelemen_albedo(s.albedo + (size_t)m.table * (kAlbedoCos * kAlbedoRough), c, rough);
+            if (lobe_u > albedo) {
+                b.lobe = LOBE_MATTE;
+                b.color = m.diff_tex >= 0 ? tex_read(s, m.diff_tex, su, sv) : m.diff;
+                b.rough = 0.f;
+            }
+        }
+        return b;
+    }
+    if (m.type == MAT_METAL) {                                         // metalMaterial.cpp:32-62
+        float costheta = dot(V, N);
+        float3 sc = mk(schlick(costheta, m.spec.x), schlick(costheta, m.spec.y), schlick(costheta, m.spec.z));
+        float rough = lobe_u > m.mix ? m.rough : m.rough_b;
+        if (matte_path) rough = rough * (1.f - kCausticBlur) + kCausticBlur;
+        b.lobe = LOBE_SPEC;
+        b.color = sc * m.gain;
+        b.rough = rough;
+        return b;
+    }
+    b.lobe = LOBE_CONSTANT;
+    b.color = mk(0.f, 0.f, 0.f);
+    b.rough = 0.f;
+    return b;
+}
+
+// ------------------------------------------------------------------ lights
+struct LightSample { float3 dir; float maxt; float pdf; float3 color; };
+
+AUR_HD bool light_visible(const Light& l, float3 P, float3 N) {       // squareLight.h:99-110
+    if (l.type == LIGHT_SQUARE) {
+        for (int i = 0; i < 4; ++i)
+            if (dot(l.p[i] - P, N) > 0.f) return true;
+        return false;
+    }
+    return dot(l.center - P, N) > -l.radius;
+}
+
+AUR_HD float3 xform_point(const float* m, float3 p) {                   // transform.cpp:196-204
+    float xp = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
+    float yp = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
+    float zp = m[8] * p.x + m[9] * p.y + m[10] * p.z + m[11];
+    float wp = m[12] * p.x + m[13] * p.y + m[14] * p.z + m[15];
+    if (wp == 1.f) return mk(xp, yp, zp);
+    return cdiv(mk(xp, yp, zp), wp);
+}
+
+// Sphere: distance along a unit ray to the near surface (tangent point if it misses).
+AUR_HD float sphere_hit(float3 c, float radius, float3 o, float3 d, float mint, float* t_out) {
+    float3 oc = o - c;
+    float b = dot(oc, d);
+    float cc = dot(oc, oc) - radius * radius;
+    float disc = b * b - cc;
+    if (disc < 0.f) { *t_out = -b; return false; }
+    float sq = sqrtf(disc);
+    float t = -b - sq;
+    if (t < mint) t = -b + sq;
+    *t_out = t;
+    return t >= mint;
+}
+AUR_HD float sphere_cone_cos(const Light& l, float3 P) {
+    float3 wc = l.center - P;
+    float dc2 = dot(wc, wc);
+    float s2 = l.radius * l.radius / dc2;
+    return sqrtf(fmaxf(0.f, 1.f - s2));
+}
+
+AUR_HD LightSample light_sample(const Light& l, float3 P, float u1, float u2) {
+    LightSample s;
+    if (l.type == LIGHT_SQUARE) {                                        // squareLight.h:57-82
+        float3 lp = mk((u1 - 0.5f) * l.xs * 2.f, (u2 - 0.5f) * l.ys * 2.f, 0.f);
+        lp = xform_point(l.m, lp);
+        float3 dir = lp - P;
+        float len = length(dir);
+        dir = normalize(dir);
+        s.dir = dir;
+        s.maxt = len - kRayBias * 10.f;
+        float d = dot(l.n, -dir);
+        if (!(d > 0.f)) d = 0.f;
+        s.color = l.le;
+        s.pdf = d == 0.f ? 0.f : (len * len) / (d * l.xs * l.ys * 4.f);
+        return s;
+    }
+    float3 wc = l.center - P;                                            // sphere (extension)
+    float dc = length(wc);
+    s.color = l.le;
+    if (dc <= l.radius) { s.dir = mk(0.f, 1.f, 0.f); s.maxt = 0.f; s.pdf = 0.f; return s; }
+    float3 w = cdiv(wc, dc);
+    float cosmax = sphere_cone_cos(l, P);
+    float cost = (1.f - u1) + u1 * cosmax;
+    float sint = sqrtf(fmaxf(0.f, 1.f - cost * cost));
+    float phi = 2.f * kPi * u2;
+    float3 dir = normalize(tangent_to_world(mk(sint * cosf(phi), sint * sinf(phi), cost), w));
+    float t;
+    sphere_hit(l.center, l.radius, P, dir, 0.f, &t);
+    s.dir = dir;
+    s.maxt = t - kRayBias * 10.f;
+    float solid = 2.f * kPi * (1.f - cosmax);
+    s.pdf = solid > 0.f ? 1.f / solid : 0.f;
+    return s;
+}
+
+// SquareLight::pdf (squareLight.h:88-97): hits the two light triangles, shortens
+// the ray to the light and returns the solid-angle pdf (two-sided, as in the reference).
+AUR_HD float light_pdf(const Light& l, float3 o, float3 d, float mint, float* maxt) {
+    if (l.type == LIGHT_SQUARE) {
+        float t, b1, b2;
+        bool hit = tri_intersect(l.p[0], xsub(l.p[1], l.p[0]), xsub(l.p[3], l.p[0]), o, d, mint, *maxt, &t, &b1, &b2);
+        if (!hit) hit = tri_intersect(l.p[2], xsub(l.p[1], l.p[2]), xsub(l.p[3], l.p[2]), o, d, mint, *maxt, &t, &b1, &b2);
+        if (!hit) return 0.f;
+        *maxt = t;
+        float dd = dot(l.n, normalize(d));
+        dd = dd > 0.f ? dd : (dd < 0.f ? -dd : 0.f);
+        float pdf = (t * t) / (dd * l.xs * l.ys * 4.f);
+        *maxt -= kRayBias * 10.f;
+        return pdf;
+    }
+    float t;
+    if (!sphere_hit(l.center, l.radius, o, d, mint, &t) || t > *maxt) return 0.f;
+    float3 wc = l.center - o;
+    if (dot(wc, wc) <= l.radius * l.radius) return 0.f;
+    *maxt = t - kRayBias * 10.f;
+    float solid = 2.f * kPi * (1.f - sphere_cone_cos(l, o));
+    return solid > 0.f ? 1.f / solid : 0.f;
+}
+
+AUR_HD float power_heuristic(float f, float g) { return (f * f) / (f * f + g * g); }  // integrator.cpp:28-31
+
+// Shading frame at a hit (embreeAccelerator.cpp:54-90 + integrator.cpp:132-150):
+// interpolated, face-forwarded, normalised normal; V = -normalize(dir); back-facing fix.
+struct Frame { float3 P, V, N; float su, sv; int attr; };
+AUR_HD Frame hit_frame(const ShadeScene& s, int prim, float t, float u, float v, float3 o, float3 d, bool need_uv) {
+    Frame f;
+    const float* n = s.corner_n + (size_t)prim * 9;
+    float w = 1.f - u - v;
+    float3 nn = mk(w * n[0] + u * n[3] + v * n[6],
+                   w * n[1] + u * n[4] + v * n[7],
+                   w * n[2] + u * n[5] + v * n[8]);
+    if (dot(nn, d) > 0.f) nn *= -1.f;
+    f.N = normalize(nn);
+    f.P = o + d * t;
+    f.attr = s.tri_attr[prim];
+    f.su = f.sv = 0.f;
+    if (need_uv && s.corner_uv) {
+        const float* uv = s.corner_uv + (size_t)prim * 6;
+        f.su = w * uv[0] + u * uv[2] + v * uv[4];
+        f.sv = w * uv[1] + u * uv[3] + v * uv[5];
+    }
+    f.V = -normalize(d);
+    if (dot(f.V, f.N) <= 0.f) {
+        float3 tmp = cross(f.N, f.V);
+        f.N = normalize(cross(f.V, tmp));
+    }
+    return f;
+}
+
+}  // namespace aur

@@ -1,0 +1,112 @@
+// aur_traverse.cuh — closest-hit and any-hit traversal of the device BVH.
+//
+// Replaces EmbreeAccelerator::intersect / intersectBinary
+// (Aurora/src/geometry/embreeAccelerator.cpp:41-100): closest hit in
+// [mint, maxt] returning (t, u, v, prim) with Embree's barycentric convention
+// (u weights vertex 1, v vertex 2), and occlusion anywhere in [mint, maxt].
+// Nodes and triangles are fetched with 128-bit read-only loads; the traversal
+// stack lives in registers/local memory (64 entries, ample for PLOC trees).
+// The triangle test is the exact FP32 Moller-Trumbore of tri_intersect, so the
+// closest prim equals a brute-force scan's whenever the minimum is unique.
+#pragma once
+#include "aur_bvh.cuh"
+#include "aur_shading.cuh"
+
+namespace aur {
+
+struct Hit { float t, u, v; int prim; };
+
+// Work counters of one or more traversals: interior-node visits (one 64-byte
+// record each) and triangle tests (one 48-byte record each). Kernels that do
+// not store them let the compiler drop the increments.
+struct TraceWork { uint32_t nodes = 0, tris = 0; };
+
+constexpr int kTraversalStack = 64;
+
+__device__ __forceinline__ float safe_rcp(float x) {
+    return __frcp_rn(fabsf(x) > 1e-20f ? x : copysignf(1e-20f, x));
+}
+
+// Slab test against one child box; tmin/tmax already carry the rounding slack.
+__device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy, float loz, float hiz,
+                                     float3 id, float3 ood, float tmin, float tmax, float* tnear) {
+    const float x0 = fmaf(lox, id.x, -ood.x), x1 = fmaf(hix, id.x, -ood.x);
+    const float y0 = fmaf(loy, id.y, -ood.y), y1 = fmaf(hiy, id.y, -ood.y);
+    const float z0 = fmaf(loz, id.z, -ood.z), z1 = fmaf(hiz, id.z, -ood.z);
+    const float tn = fmaxf(fmaxf(fminf(x0, x1), fminf(y0, y1)), fmaxf(fminf(z0, z1), tmin));
+    const float tf = fminf(fminf(fmaxf(x0, x1), fmaxf(y0, y1)), fminf(fmaxf(z0, z1), tmax));
+    *tnear = tn;
+    return tn <= tf;
+}
+
+// kAnyHit=false: closest hit, returns true when hit->prim >= 0.
+// kAnyHit=true : returns true as soon as any triangle is hit in [mint, maxt].
+template <bool kAnyHit>
+__device__ __forceinline__ bool bvh_trace(const BvhNode* __restrict__ nodes, const BvhTri* __restrict__ tris,
+                                          float3 o, float3 d, float mint, float maxt, Hit* hit, TraceWork& work) {
+    const float3 id = mk(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    const float3 ood = mk(o.x * id.x, o.y * id.y, o.z * id.z);
+    const float box_tmin = mint > 0.f ? mint * 0.99999905f : mint * 1.00000095f;
+    float tbest = maxt;
+    float box_tmax = tbest * 1.00000095f;
+    int best = -1;
+    float bu = 0.f, bv = 0.f;
+    int stack[kTraversalStack];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        if (node >= 0) {
+            ++work.nodes;
+            const float4 a = __ldg(&nodes[node].a);
+            const float4 b = __ldg(&nodes[node].b);
+            const float4 c = __ldg(&nodes[node].c);
+            const float4 e = __ldg(&nodes[node].d);
+            float t0, t1;
+            const bool h0 = slab(a.x, a.y, a.z, a.w, c.x, c.y, id, ood, box_tmin, box_tmax, &t0);
+            const bool h1 = slab(b.x, b.y, b.z, b.w, c.z, c.w, id, ood, box_tmin, box_tmax, &t1);
+            const int r0 = __float_as_int(e.x), r1 = __float_as_int(e.y);
+            if (h0 && h1) {
+                const bool first0 = t0 <= t1;
+                if (sp < kTraversalStack) stack[sp++] = first0 ? r1 : r0;   // depth <= 63 is checked at build
+                node = first0 ? r0 : r1;
+                continue;
+            }
+            if (h0) { node = r0; continue; }
+            if (h1) { node = r1; continue; }
+        } else {
+            const int packed = ~node;
+            const int start = packed >> 5, end = start + (packed & 31);
+            for (int k = start; k < end; ++k) {
+                ++work.tris;
+                const float4 p = __ldg(&tris[k].p1);
+                const float4 e1 = __ldg(&tris[k].e1);
+                const float4 e2 = __ldg(&tris[k].e2);
+                float t, u, v;
+                if (tri_intersect(mk(p.x, p.y, p.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), o, d, mint, tbest,
+                                  &t, &u, &v)) {
+                    if (kAnyHit) return true;
+                    tbest = t; bu = u; bv = v;
+                    best = __float_as_int(p.w);
+                    box_tmax = tbest * 1.00000095f;
+                }
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    if (kAnyHit) return false;
+    hit->t = tbest; hit->u = bu; hit->v = bv; hit->prim = best;
+    return best >= 0;
+}
+
+__device__ __forceinline__ bool bvh_closest(const BvhNode* nodes, const BvhTri* tris, float3 o, float3 d, float mint,
+                                            float maxt, Hit* hit, TraceWork& work) {
+    return bvh_trace<false>(nodes, tris, o, d, mint, maxt, hit, work);
+}
+__device__ __forceinline__ bool bvh_occluded(const BvhNode* nodes, const BvhTri* tris, float3 o, float3 d, float mint,
+                                             float maxt, TraceWork& work) {
+    Hit h;
+    return bvh_trace<true>(nodes, tris, o, d, mint, maxt, &h, work);
+}
+
+}  // namespace aur

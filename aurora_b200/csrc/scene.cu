@@ -1,0 +1,352 @@
+// scene.cu — flattened scenes on the device and the render entry points.
+//
+// aur_scene_create takes the camera-space soup that
+// Renderer::buildRenderEnvironment produces (Aurora/src/frontend/renderer.cpp:99-145):
+// objects then light shapes, per-corner normals/uvs (EmbreeMesh, embreeMesh.h:30-63),
+// AttributeState {material, emission} per object/light, materials, lights.
+#include "aur_capi_internal.h"
+#include <cmath>
+#include <cstring>
+
+using namespace aur;
+
+#define CUDA_TRY(x, where) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return cuda_fail(e_, where); } while (0)
+
+namespace aur {
+
+aur_status bvh_options(const aur_bvh_opts* o, BvhBuildOptions* out) {
+    *out = BvhBuildOptions();
+    if (!o) return AUR_OK;
+    if (o->max_leaf) out->max_leaf = o->max_leaf;
+    if (o->cost_traverse > 0.f) out->cost_traverse = o->cost_traverse;
+    if (o->cost_intersect > 0.f) out->cost_intersect = o->cost_intersect;
+    if (o->ploc_radius) out->ploc_radius = o->ploc_radius;
+    if (out->max_leaf < 1 || out->max_leaf > 31) return fail(AUR_ERR_INVALID_ARG, "bvh options: max_leaf must be 1..31");
+    if (out->ploc_radius < 1 || out->ploc_radius > 32)
+        return fail(AUR_ERR_INVALID_ARG, "bvh options: ploc_radius must be 1..32");
+    return AUR_OK;
+}
+
+// Square light set-up of SquareLight's constructor (squareLight.cpp:20-52).
+static Light make_light(const aur_light_desc& d) {
+    Light l;
+    memset(&l, 0, sizeof(l));
+    l.type = d.type;
+    const float inten = powf(2.f, d.exposure);
+    l.le = mk(d.color[0] * inten, d.color[1] * inten, d.color[2] * inten);
+    for (int k = 0; k < 16; ++k) l.m[k] = d.object_to_camera[k];
+    if (d.type == AUR_LIGHT_SQUARE) {
+        l.xs = d.size_x;
+        l.ys = d.size_y;
+        l.p[0] = xform_point(l.m, mk(-l.xs, -l.ys, 0.f));
+        l.p[1] = xform_point(l.m, mk(-l.xs, l.ys, 0.f));
+        l.p[2] = xform_point(l.m, mk(l.xs, l.ys, 0.f));
+        l.p[3] = xform_point(l.m, mk(l.xs, -l.ys, 0.f));
+        l.n = normalize(cross(l.p[0] - l.p[1], l.p[1] - l.p[2]));
+    } else {
+        l.center = mk(d.center[0], d.center[1], d.center[2]);
+        l.radius = d.radius;
+    }
+    return l;
+}
+
+static Material make_material(const aur_material_desc& d) {
+    Material m;
+    memset(&m, 0, sizeof(m));
+    m.type = d.type;
+    m.diff_tex = d.diffuse_tex;
+    m.spec_tex = d.specular_tex;
+    m.rough_tex = d.roughness_tex;
+    m.diff = mk(d.diffuse[0], d.diffuse[1], d.diffuse[2]);
+    m.spec = mk(d.specular[0], d.specular[1], d.specular[2]);
+    m.gain = mk(d.gain[0], d.gain[1], d.gain[2]);
+    m.rough = d.roughness;
+    m.rough_b = d.roughness_b;
+    m.refl = d.reflectance;
+    m.mix = d.mix;
+    m.table = d.type == AUR_MAT_KELEMEN ? kelemen_index(d.reflectance) : 0;
+    return m;
+}
+
+template <typename T>
+static cudaError_t upload(T** dst, const void* src, size_t count, cudaStream_t s) {
+    *dst = nullptr;
+    if (!src || count == 0) return cudaSuccess;
+    cudaError_t e = cudaMalloc((void**)dst, sizeof(T) * count);
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyAsync(*dst, src, sizeof(T) * count,
+                           is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
+}
+
+static void scene_free(aur_scene* sc) {
+    cudaStream_t s = sc->ctx->stream;
+    cudaStreamSynchronize(s);
+    bvh_free_device(&sc->bvh.bvh, s);
+    cudaStreamSynchronize(s);
+    void* bufs[] = {sc->bvh.tri_attr, sc->corner_n, sc->corner_uv, sc->attrs, sc->mats, sc->lights, sc->texs, sc->texels};
+    for (void* b : bufs) if (b) cudaFree(b);
+    delete sc;
+}
+
+}  // namespace aur
+
+DevScene aur_scene::dev() const {
+    DevScene d;
+    d.nodes = bvh.bvh.nodes;
+    d.tris = bvh.bvh.tris;
+    d.sh.mats = mats;
+    d.sh.attrs = attrs;
+    d.sh.lights = lights;
+    d.sh.texs = texs;
+    d.sh.texels = texels;
+    d.sh.albedo = ctx->kelemen;
+    d.sh.corner_n = corner_n;
+    d.sh.corner_uv = corner_uv;
+    d.sh.tri_attr = bvh.tri_attr;
+    d.sh.nlights = (int)h_lights.size();
+    d.cam = cam;
+    return d;
+}
+
+extern "C" {
+
+aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh_opts* bvh_opts, aur_scene** out) {
+    if (!ctx || !d || !out) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: NULL argument");
+    *out = nullptr;
+    if (!d->verts || !d->tri_vidx || !d->tri_attr || !d->corner_normals || d->ntri == 0)
+        return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: geometry arrays missing or empty");
+    if (!d->attr_material || !d->attr_emission || d->nattr == 0)
+        return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: attribute arrays missing");
+    if (!d->materials || d->nmat == 0) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: no materials");
+    if (d->nlight && !d->lights) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: lights missing");
+    if (d->width <= 0 || d->height <= 0 || (long long)d->width * d->height > (1ll << 31) / 4)
+        return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: bad resolution");
+    if (d->ntex && (!d->tex_dims || !d->texels)) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: textures missing");
+    // host-side validation of indices (device-resident inputs are trusted)
+    const bool host_attr = !is_device_ptr(d->tri_attr);
+    if (host_attr)
+        for (uint32_t i = 0; i < d->ntri; ++i)
+            if (d->tri_attr[i] < 0 || (uint32_t)d->tri_attr[i] >= d->nattr)
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: triangle attribute out of range");
+    for (uint32_t i = 0; i < d->nattr; ++i)
+        if (!is_device_ptr(d->attr_material) && (d->attr_material[i] < 0 || (uint32_t)d->attr_material[i] >= d->nmat))
+            return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: attribute material out of range");
+    std::vector<Texture> texs(d->ntex);
+    uint32_t texel_floats = 0;
+    for (uint32_t t = 0; t < d->ntex; ++t) {
+        const int w = d->tex_dims[2 * t], h = d->tex_dims[2 * t + 1];
+        if (w <= 0 || h <= 0) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: bad texture size");
+        texs[t].w = w; texs[t].h = h; texs[t].offset = (int)texel_floats; texs[t].pad = 0;
+        texel_floats += 3u * (uint32_t)w * (uint32_t)h;
+    }
+    std::vector<Material> mats(d->nmat);
+    for (uint32_t m = 0; m < d->nmat; ++m) {
+        const aur_material_desc& md = d->materials[m];
+        if (md.type < AUR_MAT_MATTE || md.type > AUR_MAT_CONSTANT)
+            return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: unknown material type");
+        const int tx[3] = {md.diffuse_tex, md.specular_tex, md.roughness_tex};
+        for (int k = 0; k < 3; ++k)
+            if (tx[k] >= (int)d->ntex || tx[k] < -1) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: texture index");
+        mats[m] = make_material(md);
+    }
+    std::vector<Light> lights(d->nlight);
+    for (uint32_t l = 0; l < d->nlight; ++l) {
+        if (d->lights[l].type != AUR_LIGHT_SQUARE && d->lights[l].type != AUR_LIGHT_SPHERE)
+            return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: unknown light type");
+        lights[l] = make_light(d->lights[l]);
+    }
+
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    aur_bvh* tmp = nullptr;
+    aur_status st = aur_bvh_build(ctx, d->verts, d->nvert, d->tri_vidx, d->tri_attr, d->ntri, bvh_opts, &tmp);
+    if (st != AUR_OK) return st;
+    aur_scene* sc = new aur_scene();
+    sc->ctx = ctx;
+    sc->bvh = *tmp;
+    sc->bvh.owned_by_scene = true;
+    delete tmp;
+    sc->ntri = d->ntri;
+    sc->nattr = d->nattr;
+    sc->ntexel_floats = texel_floats;
+    sc->h_mats = mats;
+    sc->h_lights = lights;
+    sc->h_texs = texs;
+    sc->cam.fov = d->fov;
+    sc->cam.w = d->width;
+    sc->cam.h = d->height;
+    std::vector<Attr> attrs(d->nattr);
+    {
+        std::vector<int32_t> am(d->nattr);
+        std::vector<float> ae(3 * d->nattr);
+        cudaMemcpy(am.data(), d->attr_material, sizeof(int32_t) * d->nattr, cudaMemcpyDefault);
+        cudaMemcpy(ae.data(), d->attr_emission, sizeof(float) * 3 * d->nattr, cudaMemcpyDefault);
+        for (uint32_t i = 0; i < d->nattr; ++i) { attrs[i].material = am[i]; attrs[i].emission = mk(ae[3 * i], ae[3 * i + 1], ae[3 * i + 2]); }
+    }
+    cudaError_t e = cudaSuccess;
+    for (const Material& m : mats)
+        if (m.type == MAT_KELEMEN && e == cudaSuccess) e = ctx_kelemen_ensure(ctx, m.table);
+    if (e == cudaSuccess) e = upload(&sc->corner_n, d->corner_normals, 9 * (size_t)d->ntri, s);
+    if (e == cudaSuccess) e = upload(&sc->corner_uv, d->corner_uvs, 6 * (size_t)d->ntri, s);
+    if (e == cudaSuccess) e = upload(&sc->attrs, attrs.data(), attrs.size(), s);
+    if (e == cudaSuccess) e = upload(&sc->mats, mats.data(), mats.size(), s);
+    if (e == cudaSuccess) e = upload(&sc->lights, lights.data(), lights.size(), s);
+    if (e == cudaSuccess) e = upload(&sc->texs, texs.data(), texs.size(), s);
+    if (e == cudaSuccess) e = upload(&sc->texels, d->texels, texel_floats, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) { scene_free(sc); return cuda_fail(e, "aur_scene_create"); }
+    *out = sc;
+    return AUR_OK;
+}
+
+aur_status aur_scene_destroy(aur_scene* sc) {
+    if (!sc) return AUR_OK;
+    DeviceGuard g(sc->ctx->device);
+    scene_free(sc);
+    return AUR_OK;
+}
+
+aur_status aur_scene_info(const aur_scene* sc, int32_t* w, int32_t* h, uint32_t* ntri, uint32_t* nmat,
+                          uint32_t* ntexel) {
+    if (!sc) return fail(AUR_ERR_INVALID_ARG, "aur_scene_info: NULL scene");
+    if (w) *w = sc->cam.w;
+    if (h) *h = sc->cam.h;
+    if (ntri) *ntri = sc->ntri;
+    if (nmat) *nmat = (uint32_t)sc->h_mats.size();
+    if (ntexel) *ntexel = sc->ntexel_floats;
+    return AUR_OK;
+}
+
+aur_status aur_scene_bvh(aur_scene* sc, aur_bvh** b) {
+    if (!sc || !b) return fail(AUR_ERR_INVALID_ARG, "aur_scene_bvh: NULL argument");
+    *b = &sc->bvh;
+    return AUR_OK;
+}
+
+aur_status aur_scene_set_params(aur_scene* sc, const float* mp, const float* texels) {
+    if (!sc) return fail(AUR_ERR_INVALID_ARG, "aur_scene_set_params: NULL scene");
+    DeviceGuard g(sc->ctx->device);
+    cudaStream_t s = sc->ctx->stream;
+    if (mp) {
+        std::vector<float> h(4 * sc->h_mats.size());
+        CUDA_TRY(cudaMemcpy(h.data(), mp, sizeof(float) * h.size(), cudaMemcpyDefault), "aur_scene_set_params");
+        for (size_t m = 0; m < sc->h_mats.size(); ++m) {
+            sc->h_mats[m].diff = mk(h[4 * m], h[4 * m + 1], h[4 * m + 2]);
+            sc->h_mats[m].rough = h[4 * m + 3];
+        }
+        CUDA_TRY(cudaMemcpyAsync(sc->mats, sc->h_mats.data(), sizeof(Material) * sc->h_mats.size(),
+                                 cudaMemcpyHostToDevice, s), "aur_scene_set_params");
+    }
+    if (texels && sc->ntexel_floats) {
+        CUDA_TRY(cudaMemcpyAsync(sc->texels, texels, sizeof(float) * sc->ntexel_floats, cudaMemcpyDefault, s),
+                 "aur_scene_set_params");
+    }
+    CUDA_TRY(cudaStreamSynchronize(s), "aur_scene_set_params");
+    return AUR_OK;
+}
+
+aur_status aur_scene_get_params(aur_scene* sc, float* mp, float* texels) {
+    if (!sc) return fail(AUR_ERR_INVALID_ARG, "aur_scene_get_params: NULL scene");
+    DeviceGuard g(sc->ctx->device);
+    if (mp) {
+        std::vector<float> h(4 * sc->h_mats.size());
+        for (size_t m = 0; m < sc->h_mats.size(); ++m) {
+            h[4 * m] = sc->h_mats[m].diff.x; h[4 * m + 1] = sc->h_mats[m].diff.y;
+            h[4 * m + 2] = sc->h_mats[m].diff.z; h[4 * m + 3] = sc->h_mats[m].rough;
+        }
+        CUDA_TRY(cudaMemcpy(mp, h.data(), sizeof(float) * h.size(), cudaMemcpyDefault), "aur_scene_get_params");
+    }
+    if (texels && sc->ntexel_floats)
+        CUDA_TRY(cudaMemcpy(texels, sc->texels, sizeof(float) * sc->ntexel_floats, cudaMemcpyDefault),
+                 "aur_scene_get_params");
+    return AUR_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ render
+namespace aur {
+
+aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathParams* p) {
+    if (!o) return fail(AUR_ERR_INVALID_ARG, "render: options are NULL");
+    if (o->spp <= 0) return fail(AUR_ERR_INVALID_ARG, "render: spp must be positive");
+    if (o->max_depth < 1 || o->max_depth > 400) return fail(AUR_ERR_INVALID_ARG, "render: max_depth must be 1..400");
+    if (o->sample_offset < 0 || (long long)o->sample_offset + o->spp > (1 << 20))
+        return fail(AUR_ERR_INVALID_ARG, "render: sample indices must stay below 2^20");
+    p->max_depth = o->max_depth;
+    p->min_depth = o->min_depth;
+    p->spp = o->spp;
+    p->sample_offset = o->sample_offset;
+    p->seed = o->seed;
+    (void)sc;
+    return AUR_OK;
+}
+
+}  // namespace aur
+
+static aur_status render_plain_impl(aur_scene* sc, const aur_render_opts* o, void* film, bool f64,
+                                    aur_render_stats* stats) {
+    if (!sc || !o || !film) return fail(AUR_ERR_INVALID_ARG, "aur_render: NULL argument");
+    PathParams p;
+    aur_status st = render_options(sc, o, &p);
+    if (st != AUR_OK) return st;
+    DeviceGuard g(sc->ctx->device);
+    cudaStream_t s = sc->ctx->stream;
+    const size_t npix = (size_t)sc->cam.w * sc->cam.h;
+    DevOut fo, fo64;
+    double* d64 = nullptr;
+    float4* f32 = nullptr;
+    if (f64) {
+        CUDA_TRY(fo64.init(film, sizeof(double) * 4 * npix, 8, s), "aur_render(film)");
+        d64 = (double*)fo64.ptr;
+        CUDA_TRY(cudaMallocAsync(&f32, sizeof(float4) * npix, s), "aur_render(film)");
+    } else {
+        const bool fp64_acc = o->fp64_film != 0;
+        CUDA_TRY(fo.init(film, sizeof(float4) * npix, 16, s), "aur_render(film)");
+        f32 = (float4*)fo.ptr;
+        if (fp64_acc) CUDA_TRY(cudaMallocAsync(&d64, sizeof(double) * 4 * npix, s), "aur_render(film)");
+    }
+    CUDA_TRY(cudaMemsetAsync(sc->ctx->counters, 0, sizeof(unsigned long long) * 8, s), "aur_render");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    cudaError_t e = launch_render_plain(sc->dev(), p, f32, d64, sc->ctx->counters, o->count_work != 0, s);
+    cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = f64 ? fo64.finish() : fo.finish();
+    unsigned long long cnt[6] = {0, 0, 0, 0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, sc->ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (f64) cudaFreeAsync(f32, s);
+    else if (d64) cudaFreeAsync(d64, s);
+    if (e != cudaSuccess) return cuda_fail(e, "aur_render");
+    if (stats) {
+        stats->camera_rays = cnt[0];
+        stats->closest_rays = cnt[1];
+        stats->shadow_rays = cnt[2];
+        stats->paths = cnt[3];
+        stats->node_visits = cnt[4];
+        stats->tri_tests = cnt[5];
+        stats->launches = 1;
+        stats->kernel_ms = ms;
+    }
+    return AUR_OK;
+}
+
+extern "C" {
+
+aur_status aur_render(aur_scene* sc, const aur_render_opts* o, float* film, aur_render_stats* stats) {
+    if (o && o->mode == AUR_RENDER_WAVEFRONT) return aur::render_wavefront(sc, o, film, stats);
+    if (o && o->mode != AUR_RENDER_PLAIN) return fail(AUR_ERR_INVALID_ARG, "aur_render: unknown mode");
+    return render_plain_impl(sc, o, film, false, stats);
+}
+
+aur_status aur_render_f64(aur_scene* sc, const aur_render_opts* o, double* film, aur_render_stats* stats) {
+    return render_plain_impl(sc, o, film, true, stats);
+}
+
+}  // extern "C"

@@ -1,0 +1,327 @@
+#!/usr/bin/env python
+"""Path samples/s of the Aurora path-tracing core on the large terrain workload
+(1920x1080, 64 spp, depth 8, roulette from the third bounce, ~3.4M triangles).
+
+One step = one full frame (W*H*spp camera paths) rendered through the C ABI.
+`value` is device-timed (CUDA events on the library's stream, inputs resident);
+`e2e` runs the public API from host arrays to a host image every step
+(scene upload + device BVH build + render + film download). Prints ONE JSON line
+on rank 0. `--impl reference` times the CPU restatement of the reference path
+(oracle/) on all host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "path samples/s at 1080p d8 (batched vs plain GPU) + adjoint/forward time ratio"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--small", action="store_true", help="reduced workload (smoke runs only)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--mode", default="auto", choices=["auto", "plain", "wavefront"])
+    return p.parse_args()
+
+
+def workload(small: bool):
+    from aurora_b200 import scenes
+    if small:
+        return scenes.terrain_scene(480, 270, spp=8, grid=257, spheres=64, sphere_level=3)
+    return scenes.terrain_scene()
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(device), f"--query-gpu={self.Q}",
+                                       "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                      stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = [l.split(",") for l in open(self.f.name).read().strip().splitlines() if l.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1])); mx = max(mx, float(r[2]))
+                for k, name in enumerate(names):
+                    if r[5 + k].strip().lower() == "active":
+                        reasons.add(name)
+            except Exception:
+                pass
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def render_opts_for(data, mode, rank=0, count_work=0, spp=None):
+    import aurora_b200 as ab
+    r = data.render
+    s = spp or r["spp"]
+    return ab.render_opts(s, r["max_depth"], r["min_depth"], r["seed"], mode=mode, sample_offset=rank * s,
+                          count_work=count_work)
+
+
+def cpu_baseline(data, tables, budget_s=15.0):
+    """CPU restatement (oracle, all host threads) on a bounded sample: a band of full-width
+    rows at the workload's spp. Returns (paths/s, sample description, cores, build seconds)."""
+    from oracle import oracle
+    cores = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    osc = oracle.OracleScene(data, tables, use_bvh=True)
+    build_s = time.perf_counter() - t0
+    r = data.render
+    W, H = data.width, data.height
+    # calibrate on one row, then size the band to the budget
+    y = H // 2
+    t0 = time.perf_counter()
+    osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y, W, 1), threads=cores, want_m2=False)
+    one = max(time.perf_counter() - t0, 1e-3)
+    rows = int(max(1, min(H // 2, budget_s / one)))
+    y0 = max(0, y - rows // 2)
+    t0 = time.perf_counter()
+    osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y0, W, rows), threads=cores,
+               want_m2=False)
+    dt = time.perf_counter() - t0
+    paths = W * rows * r["spp"]
+    return paths / dt, f"{W}x{rows} rows at y={y0} x {r['spp']} spp ({paths} paths, {dt:.1f} s)", cores, build_s
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from oracle import oracle
+    data = workload(args.small)
+    tables = np.stack([oracle.kelemen_table(k / 20.0, 20000) for k in range(21)])
+    cores = os.cpu_count() or 1
+    osc = oracle.OracleScene(data, tables, use_bvh=True)
+    r = data.render
+    W, H = data.width, data.height
+    t0 = time.perf_counter()
+    osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, H // 2, W, 1), threads=cores,
+               want_m2=False)
+    one = max(time.perf_counter() - t0, 1e-3)
+    rows = int(max(1, min(H // 4, 20.0 / max(args.steps + args.warmup, 1) / one)))
+    for _ in range(args.warmup):
+        osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, 0, W, 1), threads=cores,
+                   want_m2=False)
+    times = []
+    for k in range(args.steps):
+        y0 = (k * rows) % max(1, H - rows)
+        t0 = time.perf_counter()
+        osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y0, W, rows), threads=cores,
+                   want_m2=False)
+        times.append(time.perf_counter() - t0)
+    paths = W * rows * r["spp"]
+    ms = 1000 * statistics.mean(times)
+    value = paths / (ms / 1000)
+    sample = f"{W}x{rows} full-width rows x {r['spp']} spp per step ({paths} paths)"
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
+            "config": {"workload": f"terrain {data.ntri} tris {W}x{H} {r['spp']}spp depth {r['max_depth']}",
+                       "sample": sample},
+            "cpu_baseline": {"value": value, "unit": "path samples/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": value, "unit": "path samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import aurora_b200 as ab
+    from aurora_b200 import _abi
+
+    rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    data = workload(args.small)
+    W, H, spp = data.width, data.height, data.render["spp"]
+    ctx = ab.Context(local)
+    stream = torch.cuda.current_stream()
+    _abi.check(_abi.lib().aur_ctx_set_stream(ctx.handle, stream.cuda_stream), "aur_ctx_set_stream")
+    t0 = time.perf_counter()
+    scene = ab.Scene(ctx, data)
+    build_s = time.perf_counter() - t0
+    film = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+
+    def frame(mode, count_work=0, spp_=None):
+        return scene.render(render_opts_for(data, mode, rank, count_work, spp_), out=film)
+
+    modes = {"plain": _abi.RENDER_PLAIN, "wavefront": _abi.RENDER_WAVEFRONT}
+    have_wf = True
+    try:
+        frame(_abi.RENDER_WAVEFRONT, spp_=1)
+    except ab.AuroraError:
+        have_wf = False
+    head = args.mode if args.mode != "auto" else ("wavefront" if have_wf else "plain")
+
+    def timed(mode, steps, warmup):
+        for _ in range(warmup):
+            frame(modes[mode])
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        kernel_ms, launches, stats = 0.0, 0, None
+        e0.record(stream)
+        for _ in range(steps):
+            res = frame(modes[mode])
+            kernel_ms += res.stats["kernel_ms"]
+            launches += res.stats["launches"]
+            stats = res.stats
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        if dist:
+            t = torch.tensor([ms, kernel_ms], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms, kernel_ms = float(t[0]), float(t[1])
+        return ms / steps, kernel_ms / steps, launches, stats
+
+    # headline mode, with clocks sampled during the timed region
+    clocks = Clocks(local)
+    ms_step, kms_step, launches, st = timed(head, args.steps, args.warmup)
+    clk = clocks.stop()
+    paths_step = W * H * spp
+    value = world * paths_step / (ms_step / 1000.0)
+    rays_step = st["closest_rays"] + st["shadow_rays"]
+
+    # the other renderer for the batched-vs-plain ratio
+    other = {}
+    if head == "wavefront":
+        pms, _, _, pst = timed("plain", max(1, args.steps // 2), 1)
+        other = {"plain_value": world * paths_step / (pms / 1000.0)}
+        other["batched_vs_plain"] = value / other["plain_value"]
+    else:
+        other = {"plain_value": value, "wavefront_value": None, "batched_vs_plain": None}
+
+    # roofline of the dominant kernel: algorithmic bytes from a counting pass (1 spp, untimed)
+    cw = frame(modes[head], count_work=1, spp_=1).stats
+    bytes_per_path = (cw["node_visits"] * 64 + cw["tri_tests"] * 48) / max(cw["paths"], 1)
+    peak, peak_kind = peaks()
+    achieved = bytes_per_path * paths_step / (kms_step / 1000.0) / 1e9
+    traffic = None
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            tj = json.load(f).get(head)
+            if tj:
+                traffic = tj["dram_bytes_per_path"] * paths_step
+    except Exception:
+        pass
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_render_plain" if head == "plain" else "wavefront",
+            "bytes_per_path": bytes_per_path,
+            "node_visits_per_path": cw["node_visits"] / max(cw["paths"], 1),
+            "tri_tests_per_path": cw["tri_tests"] / max(cw["paths"], 1)}
+
+    # end to end through the public C ABI with host buffers (scene arrays in, image out)
+    e2e = None
+    if not args.no_e2e:
+        desc_bytes = sum(a.nbytes for a in (data.verts, data.tri_vidx, data.tri_attr, data.corner_normals,
+                                            data.corner_uvs, data.attr_material, data.attr_emission))
+        host_film = np.zeros((H, W, 4), np.float32)
+        e2e_steps = max(1, min(args.steps, 2))
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(e2e_steps):
+            sc2 = ab.Scene(ctx, data)
+            sc2.render(render_opts_for(data, modes[head], rank), out=host_film)
+            sc2.close()
+        torch.cuda.synchronize()
+        dt = (time.perf_counter() - t0) / e2e_steps
+        if dist:
+            t = torch.tensor([dt], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            dt = float(t[0])
+        e2e = {"value": world * paths_step / dt, "unit": "path samples/s", "h2d_bytes_per_step": int(desc_bytes),
+               "d2h_bytes_per_step": int(host_film.nbytes), "ms_per_step": dt * 1000,
+               "includes": "scene upload + device BVH build + render + film download"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        tables = np.stack([ctx.kelemen_table(k / 20.0) for k in range(21)])
+        v, sample, cores, bs = cpu_baseline(data, tables)
+        cpu = {"value": v, "unit": "path samples/s", "cores": cores, "kind": "port", "sample": sample,
+               "bvh_build_s": bs}
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator, no external data)",
+                "config": {"workload": f"terrain {data.ntri} tris {W}x{H} {spp}spp depth {data.render['max_depth']} "
+                                       f"roulette>2 ({head})",
+                           "renderer": head, "l2": "inputs larger than L2 (BVH+triangles > 126 MB); no flush",
+                           "multi_gpu": "each rank renders the full frame with its own sample indices"},
+                "rays_per_s": world * rays_step / (ms_step / 1000.0), "kernel_ms_per_step": kms_step,
+                "bvh_build_s": build_s, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
+                "e2e": e2e, "clocks": clk}
+        line.update(other)
+        print(json.dumps(line), flush=True)
+    scene.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,87 @@
+"""Rendered images of the plain renderer against the CPU restatement at equal spp:
+per-pixel mean within 3 sigma (criterion c). Both sides consume the same
+counter-based random numbers, so the images agree far more tightly than 3 sigma."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def compare(gpu, mean, m2, spp, max_frac=0.005):
+    var = m2 / max(spp - 1, 1)
+    sig = np.sqrt(var / spp)
+    d = np.abs(gpu[..., :3].astype(np.float64) - mean[..., :3])
+    bad = d > 3 * sig + 1e-4 * (1 + np.abs(mean[..., :3]))
+    frac = bad.any(-1).mean()
+    assert frac <= max_frac, (frac, np.argwhere(bad.any(-1))[:5])
+    assert np.array_equal(gpu[..., 3], mean[..., 3].astype(np.float32))
+    return frac, float(d.max())
+
+
+def render_both(ctx, oracle_lib, data, tables, spp, crop=None, mode=0):
+    import aurora_b200 as ab
+    r = data.render
+    scene = ab.Scene(ctx, data)
+    res = scene.render(ab.render_opts(spp, r["max_depth"], r["min_depth"], r["seed"], mode=mode))
+    osc = oracle_lib.OracleScene(data, tables)
+    mean, m2, counts = osc.render(spp, r["max_depth"], r["min_depth"], r["seed"], crop=crop)
+    g = res.film if crop is None else res.film[crop[1]:crop[1] + crop[3], crop[0]:crop[0] + crop[2]]
+    return g, mean, m2, counts, res.stats
+
+
+def test_box_scene_256_16spp(ctx, oracle_lib, kelemen_tables):
+    from aurora_b200 import scenes
+    data = scenes.box_scene()
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16)
+    frac, dmax = compare(g, mean, m2, 16)
+    assert stats["paths"] == 256 * 256 * 16
+    assert abs(stats["closest_rays"] - int(counts[0])) <= 1e-3 * counts[0]
+    assert abs(stats["shadow_rays"] - int(counts[1])) <= 1e-3 * counts[1]
+    print(f"\nbox: {frac:.5f} of pixels beyond 3 sigma, max |diff| {dmax:.3g}")
+
+
+def test_sphere_scene_crop(ctx, oracle_lib, kelemen_tables):
+    from aurora_b200 import scenes
+    data = scenes.sphere_scene(256, 256)
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16, crop=(64, 64, 128, 128))
+    compare(g, mean, m2, 16)
+
+
+def test_texture_scene(ctx, oracle_lib, kelemen_tables):
+    from aurora_b200 import scenes
+    data = scenes.texture_scene(96, 96)
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 8)
+    compare(g, mean, m2, 8)
+
+
+def test_terrain_small(ctx, oracle_lib, kelemen_tables):
+    """The large-scene generator at reduced size (roulette, 16 materials, 4 lights, depth 8)."""
+    from aurora_b200 import scenes
+    data = scenes.terrain_scene(160, 90, grid=129, spheres=32, sphere_level=2)
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 8)
+    compare(g, mean, m2, 8)
+
+
+def test_progressive_and_fp64(ctx):
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    data = scenes.box_scene(64, 64)
+    scene = ab.Scene(ctx, data)
+    full = scene.render(ab.render_opts(16, 5, 5, 1)).film
+    a = scene.render(ab.render_opts(8, 5, 5, 1, sample_offset=0)).film
+    b = scene.render(ab.render_opts(8, 5, 5, 1, sample_offset=8)).film
+    np.testing.assert_allclose((a + b) / 2, full, rtol=1e-5, atol=1e-6)
+    f64 = scene.render_f64(ab.render_opts(16, 5, 5, 1)).film
+    np.testing.assert_allclose(f64, full, rtol=1e-5, atol=1e-6)
+    c = scene.render(ab.render_opts(16, 5, 5, 1)).film
+    assert np.array_equal(c, full)    # deterministic
+
+
+def test_invalid_options(ctx):
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    scene = ab.Scene(ctx, scenes.box_scene(16, 16))
+    for bad in (ab.render_opts(0, 5, 5, 1), ab.render_opts(4, 0, 5, 1), ab.render_opts(4, 5, 5, 1, sample_offset=-1),
+                ab.render_opts(4, 5, 5, 1, mode=7)):
+        with pytest.raises(ab.AuroraError):
+            scene.render(bad)

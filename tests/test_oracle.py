@@ -1,0 +1,201 @@
+"""Pins the CPU oracle (oracle/aurora_oracle.cpp) with hand-derived known answers.
+
+The reference ships no tests or golden vectors and cannot be built here, so the
+oracle is checked against independent float64 restatements of the reference
+formulas and against analytic light-transport integrals.
+"""
+import math
+
+import numpy as np
+import pytest
+
+
+def splitmix_u01(seed, pixel, sample, dim):
+    M = (1 << 64) - 1
+
+    def fin(z):
+        z = ((z ^ (z >> 30)) * 0xbf58476d1ce4e5b9) & M
+        z = ((z ^ (z >> 27)) * 0x94d049bb133111eb) & M
+        return z ^ (z >> 31)
+    key = fin((seed * 0x9e3779b97f4a7c15 + 0x632be59bd9b4e019) & M)
+    counter = (pixel << 32) | (sample << 12) | dim
+    z = fin((key + counter * 0x9e3779b97f4a7c15) & M)
+    return (z >> 40) / 16777216.0
+
+
+def test_rng_matches_splitmix64(oracle_lib):
+    for seed, px, s, d in [(1, 0, 0, 0), (1, 65535, 15, 41), (7, 123456, 1000, 3), (3, 2**31, 2**19, 4095)]:
+        assert oracle_lib.rng_u01(seed, px, s, d) == splitmix_u01(seed, px, s, d)
+
+
+def test_rng_uniformity(oracle_lib):
+    u = np.array([oracle_lib.rng_u01(5, p, 0, 2) for p in range(20000)])
+    assert 0.0 <= u.min() and u.max() < 1.0
+    hist, _ = np.histogram(u, bins=10, range=(0, 1))
+    assert np.all(np.abs(hist - 2000) < 6 * math.sqrt(2000))
+
+
+def tri_soup():
+    verts = np.array([[0, 0, -2], [1, 0, -2], [0, 1, -2], [0, 0, -3], [1, 0, -3], [0, 1, -3]], np.float32)
+    idx = np.array([[0, 1, 2], [3, 4, 5]], np.uint32)
+    return verts, idx
+
+
+def ray(o, d, mint=0.0, maxt=1e30):
+    return np.array([*o, mint, *d, maxt], np.float32)
+
+
+def test_moller_trumbore_known_answers(oracle_lib):
+    v, i = tri_soup()
+    rays = np.stack([ray((0.25, 0.25, 0), (0, 0, -1)),        # hits both, nearest is prim 0 at t=2
+                     ray((0.25, 0.25, 0), (0, 0, 1)),         # behind the origin
+                     ray((0.25, 0.25, 0), (1, 0, 0)),         # parallel to both
+                     ray((0.25, 0.25, 0), (0, 0, -1), 2.5),   # mint skips prim 0
+                     ray((0.25, 0.25, 0), (0, 0, -1), 0, 1.5),  # maxt before prim 0
+                     ray((0.0, 0.0, 0), (0, 0, -1)),          # exactly on a vertex (b1 = b2 = 0)
+                     ray((0.6, 0.6, 0), (0, 0, -1))])         # outside (b1 + b2 > 1)
+    hits, ties = oracle_lib.trace_brute(v, i, np.array([7, 9], np.int32), rays)
+    assert hits["prim"].tolist() == [0, -1, -1, 1, -1, 0, -1]
+    assert hits["attr"][0] == 7 and hits["attr"][3] == 9
+    assert hits["t"][0] == 2.0 and hits["t"][3] == 3.0
+    assert abs(hits["u"][0] - 0.25) < 1e-7 and abs(hits["v"][0] - 0.25) < 1e-7
+    occ = oracle_lib.occluded_brute(v, i, rays)
+    assert occ.tolist() == [1, 0, 0, 1, 0, 1, 0]
+
+
+def test_exact_ties_are_counted(oracle_lib):
+    v, i = tri_soup()
+    v2 = np.concatenate([v, v[:3]])
+    i2 = np.concatenate([i, np.array([[6, 7, 8]], np.uint32)])
+    hits, ties = oracle_lib.trace_brute(v2, i2, None, np.stack([ray((0.25, 0.25, 0), (0, 0, -1))]))
+    assert ties[0] == 2 and hits["prim"][0] == 2     # the later duplicate wins, as with maxt=t replacement
+
+
+def test_cpu_bvh_equals_brute_force(oracle_lib):
+    from aurora_b200 import scenes
+    r = np.random.default_rng(11)
+    n = 3000
+    c = r.uniform(-2, 2, (n, 1, 3))
+    verts = (c + r.normal(0, 0.15, (n, 3, 3))).reshape(-1, 3).astype(np.float32)
+    idx = np.arange(3 * n, dtype=np.uint32).reshape(-1, 3)
+    b = scenes.SceneBuilder(8, 8, 0.5)
+    m = b.material(0, diffuse=(0.5, 0.5, 0.5))
+    b.mesh(verts, idx, m)
+    data = b.build()
+    rays = scenes.sphere_rays(20000, seed=12)
+    brute, ties = oracle_lib.trace_brute(data.verts, data.tri_vidx, data.tri_attr, rays)
+    sc = oracle_lib.OracleScene(data, use_bvh=True)
+    fast = sc.trace(rays)
+    ok = ties <= 1
+    assert np.array_equal(fast["prim"][ok], brute["prim"][ok])
+    assert np.array_equal(fast["t"][ok & (brute["prim"] >= 0)], brute["t"][ok & (brute["prim"] >= 0)])
+
+
+def test_brdf_known_values(oracle_lib):
+    """Lambert and Cook-Torrance (Beckmann) against float64 restatements of lambert.h / cookTorrance.cpp."""
+    rng = np.random.default_rng(3)
+    recs, want_eval, want_pdf = [], [], []
+    for _ in range(200):
+        N = np.array([0.0, 0.0, 1.0])
+        V = rng.normal(size=3); V[2] = abs(V[2]) + 0.3; V /= np.linalg.norm(V)
+        L = rng.normal(size=3); L[2] = abs(L[2]) + 0.3; L /= np.linalg.norm(L)
+        col = rng.uniform(0.1, 0.9, 3)
+        rough = rng.uniform(0.1, 0.8)
+        H = (L + V) / np.linalg.norm(L + V)
+        vh, vn, nh, ln = V @ H, V @ N, H @ N, L @ N
+        r2 = rough * rough
+        D = 1.0 / (r2 * math.pi * nh ** 3) * math.exp(-math.tan(math.acos(nh)) ** 2 / r2)
+        ok = vh > 0.001 and ln > 0.001 and vn > 0.001
+        want_eval.append(col * D / (4 * vh * vh) if ok else np.zeros(3))
+        rr = max(0.001, r2)
+        Dp = math.exp(-math.tan(math.acos(nh)) ** 2 / rr) / (rr * math.pi * nh ** 3)
+        want_pdf.append(Dp / (4 * vh))
+        recs.append([1, *col, rough, *L, *V, *N])
+    recs = np.array(recs, np.float32)
+    ev = oracle_lib.probe(1, recs)
+    pdf = oracle_lib.probe(2, recs)[:, 0]
+    np.testing.assert_allclose(ev, np.array(want_eval), rtol=2e-5, atol=1e-7)
+    np.testing.assert_allclose(pdf, np.array(want_pdf), rtol=2e-5, atol=1e-10)
+    lam = recs.copy(); lam[:, 0] = 0
+    np.testing.assert_allclose(oracle_lib.probe(1, lam), recs[:, 1:4] / math.pi, rtol=1e-6)
+    np.testing.assert_allclose(oracle_lib.probe(2, lam)[:, 0], 0.5 / math.pi, rtol=1e-6)
+
+
+def test_ct_sample_is_a_reflection(oracle_lib):
+    rng = np.random.default_rng(5)
+    recs = []
+    for _ in range(500):
+        N = rng.normal(size=3); N /= np.linalg.norm(N)
+        V = rng.normal(size=3); V /= np.linalg.norm(V)
+        if V @ N < 0.2:
+            V = V - 2 * (V @ N) * N + 0.2 * N
+            V /= np.linalg.norm(V)
+        recs.append([1, 0.5, 0.6, 0.7, rng.uniform(0.1, 0.9), *V, *N, rng.uniform(), rng.uniform()])
+    recs = np.array(recs, np.float32)
+    out = oracle_lib.probe(0, recs)
+    L = out[:, :3].astype(np.float64)
+    np.testing.assert_allclose(np.linalg.norm(L, axis=1), 1.0, atol=1e-5)
+    V, N = recs[:, 5:8].astype(np.float64), recs[:, 8:11].astype(np.float64)
+    H = (L + V) / np.linalg.norm(L + V, axis=1, keepdims=True)
+    vh = np.sum(V * H, 1)
+    pdf = out[:, 3]
+    # sample colour = colour * D / (4 vh^2) with pdf = D / (4 vh): colour * pdf / vh
+    good = (pdf > 0) & (pdf < 1000) & (vh > 0.01) & (out[:, 4] > 0)   # samples with v.h <= 1e-4 are black (pdf 1)
+    np.testing.assert_allclose(out[good, 4], recs[good, 1] * pdf[good] / vh[good], rtol=2e-4)
+
+
+def test_camera_and_power_heuristic(oracle_lib):
+    out = oracle_lib.probe(4, np.array([[0.36397, 256, 256, 128, 128, 0.0, 0.0],
+                                        [0.36397, 256, 256, 0, 0, 0.0, 0.0]], np.float32))
+    np.testing.assert_allclose(out[0], [0, 0, -1], atol=1e-7)
+    d = np.array([-0.36397, 0.36397, -1.0]); d /= np.linalg.norm(d)
+    np.testing.assert_allclose(out[1], d, rtol=1e-6)
+    w = oracle_lib.probe(5, np.array([[2.0, 1.0], [0.5, 0.5]], np.float32))[:, 0]
+    np.testing.assert_allclose(w, [0.8, 0.5], rtol=1e-7)
+
+
+def _plane_under_light(albedo=0.6, h=1.0, s=0.25, le=(4.0, 4.0, 4.0), px=0.8):
+    from aurora_b200 import scenes
+    from aurora_b200 import _abi
+    b = scenes.SceneBuilder(16, 16, 0.01, world_to_camera=scenes.look_at((px, 3, 0.001), (px, 0, 0)))
+    m = b.material(_abi.MAT_MATTE, diffuse=(albedo,) * 3)
+    v, f = scenes.quad((-5, 0, 5), (5, 0, 5), (5, 0, -5), (-5, 0, -5))
+    b.mesh(v, f, m, normals=np.tile([0, 1, 0], (4, 1)))
+    b.square_light(scenes.translate(0, h, 0) @ scenes.rot_x(-90.0), s, s, le, 0.0)
+    return b.build()
+
+
+def test_direct_lighting_matches_the_analytic_integral(oracle_lib):
+    """Lambert plane under a square light: L = rho/pi * Le * integral cos cos' / r^2 dA (float64 quadrature)."""
+    albedo, h, s, px = 0.6, 1.0, 0.25, 0.8
+    data = _plane_under_light(albedo, h, s, px=px)
+    sc = oracle_lib.OracleScene(data, use_bvh=False)
+    mean, m2, counts = sc.render(4096, 1, 1, seed=3, crop=(8, 8, 1, 1))
+    # the pixel at (8,8) looks (straight down, tiny fov) at the plane point (px, 0, 0) beside the light
+    n = 400
+    g = (np.arange(n) + 0.5) / n * 2 * s - s
+    X, Z = np.meshgrid(g, g)
+    r2 = (X - px) ** 2 + Z ** 2 + h ** 2
+    integral = np.sum((h / np.sqrt(r2)) ** 2 / r2) * (2 * s / n) ** 2
+    want = albedo / math.pi * 4.0 * integral
+    got = mean[0, 0, 0]
+    sigma = math.sqrt(m2[0, 0, 0] / 4095) / math.sqrt(4096)
+    assert abs(got - want) < 4 * sigma + 1e-3 * want, (got, want, sigma)
+
+
+def test_oracle_render_is_deterministic(oracle_lib):
+    from aurora_b200 import scenes
+    data = scenes.box_scene(64, 64)
+    sc = oracle_lib.OracleScene(data)
+    a, _, ca = sc.render(4, 5, 5, 1, crop=(20, 20, 8, 8))
+    b, _, cb = sc.render(4, 5, 5, 1, crop=(20, 20, 8, 8))
+    assert np.array_equal(a, b) and np.array_equal(ca, cb)
+    assert np.all(a[..., 3] == 1.0) and np.all(a[..., :3] > 0)
+
+
+def test_kelemen_table_restatement(oracle_lib):
+    t0 = oracle_lib.kelemen_table(0.0, 2000)
+    t1 = oracle_lib.kelemen_table(1.0, 2000)
+    assert np.all(t0 >= 0) and np.all(t1 >= t0 - 1e-6)
+    # reflectance 1 => F = 1; at normal incidence and low roughness the estimator -> 1
+    assert abs(t1[63, 1] - 1.0) < 0.02
