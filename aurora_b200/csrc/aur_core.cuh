@@ -68,6 +68,21 @@ struct PathRng {
     AUR_HD float u(uint32_t dim) const { return rng_u01(key, base | (uint64_t)dim); }
 };
 
+// ---------------------------------------------------------------- transcendentals
+// The shading math is evaluated in double and rounded once to float, which is
+// the correctly rounded float result in all but double-rounding cases. That is
+// what the host's libm returns (to within its own <1 ulp), so device and CPU
+// restatement agree on BRDF values even where the Beckmann lobe amplifies a
+// 1-ulp difference (d ln D / d theta ~ 2 tan / m^2).
+AUR_HD float xexpf(float x) { return (float)exp((double)x); }
+AUR_HD float xlogf(float x) { return (float)log((double)x); }
+AUR_HD float xpowf(float x, float y) { return (float)pow((double)x, (double)y); }
+AUR_HD float xacosf(float x) { return (float)acos((double)x); }
+AUR_HD float xtanf(float x) { return (float)tan((double)x); }
+AUR_HD float xatanf(float x) { return (float)atan((double)x); }
+AUR_HD float xcosf(float x) { return (float)cos((double)x); }
+AUR_HD float xsinf(float x) { return (float)sin((double)x); }
+
 // ---------------------------------------------------------------- float3 helpers
 AUR_HD float3 mk(float x, float y, float z) { float3 r; r.x = x; r.y = y; r.z = z; return r; }
 AUR_HD float3 operator+(float3 a, float3 b) { return mk(a.x + b.x, a.y + b.y, a.z + b.z); }
@@ -90,9 +105,11 @@ AUR_HD float length(float3 v) {
     return l == 0.f ? 0.0001f : l;
 }
 AUR_HD float3 normalize(float3 v) { float inv = 1.f / length(v); return mk(v.x * inv, v.y * inv, v.z * inv); }
-AUR_HD float lum(float3 c) { return 0.2126f * c.x + 0.7152f * c.y + 0.0722f * c.z; }
-AUR_HD bool is_black(float3 c) { return c.x < kIsBlack && c.y < kIsBlack && c.z < kIsBlack; }
-AUR_HD float schlick(float vdoth, float refl) { return refl + powf(1.f - vdoth, 5.f) * (1.f - refl); }
+AUR_HD float lum(float3 c) { return (float)(0.2126 * c.x + 0.7152 * c.y + 0.0722 * c.z); }   // double literals
+AUR_HD bool is_black(float3 c) {   // compared with the double ISBLACK as in color.h:149-151
+    return (double)c.x < 0.0001 && (double)c.y < 0.0001 && (double)c.z < 0.0001;
+}
+AUR_HD float schlick(float vdoth, float refl) { return refl + xpowf(1.f - vdoth, 5.f) * (1.f - refl); }
 
 AUR_HD void coordinate_system(float3 v1, float3* v2, float3* v3) {
     if (!(v1.x != 0.f) && v1.y != 0.f && !(v1.z != 0.f)) *v2 = cross(v1, mk(1.f, 0.f, 0.f));
@@ -107,11 +124,12 @@ AUR_HD float3 tangent_to_world(float3 dir, float3 n) {
     r = r + n * dir.z;
     return r;
 }
+AUR_HD float two_pi_times(float r) { return (float)(6.283185307179586 * (double)r); }   // 2 * M_PI * r in double
 AUR_HD float3 sample_hemisphere_uniform(float r1, float r2) {
     float z = r1;
     float r = sqrtf(fmaxf(0.f, 1.f - z * z));
-    float phi = 2.f * kPi * r2;
-    return mk(r * cosf(phi), r * sinf(phi), z);
+    float phi = two_pi_times(r2);
+    return mk(r * xcosf(phi), r * xsinf(phi), z);
 }
 
 // Neumaier-compensated FP32 accumulator (film and gradient sums).

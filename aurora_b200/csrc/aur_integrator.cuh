@@ -97,6 +97,15 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
 
 enum RayKind : int { RAY_CAMERA = 0, RAY_DIFFUSE = 1, RAY_SPECULAR = 2 };
 
+// Firefly filter (integrator.cpp:278-281). A non-finite estimate would never
+// leave the reference's loop; it is dropped (returned as black) instead, which
+// also bounds the loop to at most ~50 iterations.
+AUR_HD float3 firefly_clamp(float3 Lo) {
+    if (!isfinite(Lo.x) || !isfinite(Lo.y) || !isfinite(Lo.z)) return mk(0.f, 0.f, 0.f);
+    for (int k = 0; k < 64 && (Lo.x > kFirefly || Lo.y > kFirefly || Lo.z > kFirefly); ++k) Lo *= 0.2f;
+    return Lo;
+}
+
 // One camera path; returns the clamped radiance, sets *alpha to 1 on a camera hit.
 __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathParams& p, int px, int py,
                                                  const PathRng& rng, RayCounts& rc, float* alpha) {
@@ -141,8 +150,7 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         ++rc.closest;
         if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) break;
     }
-    while (Lo.x > kFirefly || Lo.y > kFirefly || Lo.z > kFirefly) Lo *= 0.2f;
-    return Lo;
+    return firefly_clamp(Lo);
 }
 
 }  // namespace aur

@@ -151,10 +151,15 @@ struct Brdf {                // an instantiated lobe: BrdfState{Brdf*, bxdfParam
 };
 struct BrdfSample { float3 dir; float pdf; float3 color; float maxt; };
 
+// `albedo * M_PI_INV` with the reference's unparenthesised #define M_PI_INV 1.f/M_PI
+// (math_utils.h:26) parses as (albedo * 1.f) / M_PI, i.e. Color::operator/(float)
+// with (float)M_PI: a multiply by the float reciprocal 1/(float)pi.
+constexpr float kInvPiMacro = 1.f / 3.14159265358979323846f;
+
 AUR_HD float ct_d(float rough, float cosa, float tana) {        // cookTorrance.cpp:40-45
     float rough2 = fmaxf(0.001f, rough * rough);
-    float e = expf(-(tana * tana) / rough2);
-    float div = rough2 * kPi * powf(cosa, 3.f);
+    float e = xexpf(-(tana * tana) / rough2);
+    float div = (float)((double)rough2 * 3.141592653589793 * (double)xpowf(cosa, 3.f));   // rough2 * M_PI in double
     return e / div;
 }
 
@@ -164,15 +169,15 @@ AUR_HD BrdfSample brdf_sample(const Brdf& b, float3 V, float3 N, float r1, float
         float3 dir = sample_hemisphere_uniform(r1, r2);
         s.dir = normalize(tangent_to_world(dir, N));
         s.pdf = kInvPi * 0.5f;
-        s.color = b.color * kInvPi;
+        s.color = b.color * kInvPiMacro;
         s.maxt = 1000000.f;
         return s;
     }
     if (b.lobe == LOBE_SPEC) {                                       // cookTorrance.cpp:47-99
-        float z = cosf(atanf(b.rough * sqrtf(-logf(1.f - r1))));
+        float z = xcosf(xatanf(b.rough * sqrtf((float)(-log(1.0 - (double)r1)))));
         float r = sqrtf(fmaxf(0.f, 1.f - z * z));
-        float phi = kPi * 2.f * r2;
-        float3 dir = normalize(mk(r * cosf(phi), r * sinf(phi), z));
+        float phi = two_pi_times(r2);
+        float3 dir = normalize(mk(r * xcosf(phi), r * xsinf(phi), z));
         float3 H = normalize(tangent_to_world(dir, N));
         float vdoth = dot(V, H);
         float3 L = normalize((H * 2.f) * vdoth - V);
@@ -180,11 +185,11 @@ AUR_HD BrdfSample brdf_sample(const Brdf& b, float3 V, float3 N, float r1, float
         s.color = mk(0.f, 0.f, 0.f);
         s.pdf = 1.f;
         if (vdoth > 0.0001f) {
-            float tana = (ndoth > 0.999f) ? 0.f : tanf(acosf(ndoth));
+            float tana = (ndoth > 0.999f) ? 0.f : xtanf(xacosf(ndoth));
             float D = ct_d(b.rough, ndoth, tana);
             D = fminf(D, 1000.f);
             s.pdf = D / (4.f * vdoth);
-            s.color = b.color * (D / (4.f * vdoth * vdoth));
+            s.color = cdiv(b.color * D, 4.f * vdoth * vdoth);
             if (s.pdf > 100000.f) { s.pdf *= 0.01f; s.color *= 0.01f; }
         }
         s.dir = L;
@@ -198,16 +203,17 @@ AUR_HD BrdfSample brdf_sample(const Brdf& b, float3 V, float3 N, float r1, float
 
 AUR_HD float3 brdf_eval(const Brdf& b, float3 L, float3 V, float3 N) {
     if (b.lobe == LOBE_MATTE) {                                      // lambert.h:68-76
-        return dot(L, N) > 0.f ? b.color * kInvPi : mk(0.f, 0.f, 0.f);
+        return dot(L, N) > 0.f ? b.color * kInvPiMacro : mk(0.f, 0.f, 0.f);
     }
     if (b.lobe == LOBE_SPEC) {                                       // cookTorrance.cpp:125-144
         float3 H = normalize(L + V);
         float vdoth = dot(V, H), vdotn = dot(V, N), ndoth = dot(H, N), ldotn = dot(L, N);
         float r2 = b.rough * b.rough;
-        float ta = tanf(acosf(ndoth));
-        float D = (1.f / (r2 * kPi * powf(ndoth, 3.f))) * expf(-(ta * ta) / r2);
+        float ta = xtanf(xacosf(ndoth));
+        float D = (float)((1.f / ((double)r2 * 3.141592653589793 * (double)xpowf(ndoth, 3.f))) *
+                          (double)xexpf(-(ta * ta) / r2));
         if (vdoth <= 0.001f || ldotn <= 0.001f || vdotn <= 0.001f || isnan(D)) return mk(0.f, 0.f, 0.f);
-        return b.color * (D / (4.f * vdoth * vdoth));
+        return cdiv(b.color * D, (float)(4.0 * vdoth * vdoth));
     }
     return mk(0.f, 0.f, 0.f);
 }
@@ -217,7 +223,7 @@ AUR_HD float brdf_pdf(const Brdf& b, float3 L, float3 V, float3 N) {
     if (b.lobe == LOBE_SPEC) {                                       // cookTorrance.cpp:101-117
         float3 H = normalize(L + V);
         float vdoth = dot(V, H), ndoth = dot(N, H);
-        float D = ct_d(b.rough, ndoth, tanf(acosf(ndoth)));
+        float D = ct_d(b.rough, ndoth, xtanf(xacosf(ndoth)));
         if (isnan(D)) D = 0.f;
         return D / (4.f * vdoth);
     }
@@ -239,13 +245,16 @@ AUR_HD float kelemen_albedo(const float* table, float costheta, float roughness)
     float va = table[i * kAlbedoRough + ra];
     float vb = table[i1 * kAlbedoRough + ra];
     float mixc = costheta * (kAlbedoCos - 1) - (float)i;
-    float resA = (1.f - mixc) * va + mixc * vb;
+    float resA = (float)((1. - mixc) * va + (double)(mixc * vb));
     va = table[i * kAlbedoRough + rb];
     vb = table[i1 * kAlbedoRough + rb];
-    float resB = (1.f - mixc) * va + mixc * vb;
+    float resB = (float)((1. - mixc) * va + (double)(mixc * vb));
     float rmix = roughness * (kAlbedoRough - 1) - (float)ra;
-    return (1.f - rmix) * resA + rmix * resB;
+    return (float)((1. - rmix) * resA + (double)(rmix * resB));
 }
+
+// roughness * (1 - CAUSTIC_BLUR) + CAUSTIC_BLUR with the reference's double constants
+AUR_HD float caustic_blur(float r) { return (float)((double)r * (1.0 - 0.2) + 0.2); }
 
 // Material::getBrdf for every supported material. `lobe_u` is the vertex's
 // lobe-choice random number; `st` the interpolated uv.
@@ -261,7 +270,7 @@ AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float 
     }
     if (m.type == MAT_KELEMEN || m.type == MAT_COOKTORRANCE) {
         float rough = m.rough_tex >= 0 ? tex_read(s, m.rough_tex, su, sv).x : m.rough;
-        if (matte_path) rough = rough * (1.f - kCausticBlur) + kCausticBlur;
+        if (matte_path) rough = caustic_blur(rough);
         b.lobe = LOBE_SPEC;
         b.color = m.spec_tex >= 0 ? tex_read(s, m.spec_tex, su, sv) : m.spec;
         b.rough = rough;
@@ -281,7 +290,7 @@ AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float 
         float costheta = dot(V, N);
         float3 sc = mk(schlick(costheta, m.spec.x), schlick(costheta, m.spec.y), schlick(costheta, m.spec.z));
         float rough = lobe_u > m.mix ? m.rough : m.rough_b;
-        if (matte_path) rough = rough * (1.f - kCausticBlur) + kCausticBlur;
+        if (matte_path) rough = caustic_blur(rough);
         b.lobe = LOBE_SPEC;
         b.color = sc * m.gain;
         b.rough = rough;
@@ -337,17 +346,17 @@ AUR_HD float sphere_cone_cos(const Light& l, float3 P) {
 AUR_HD LightSample light_sample(const Light& l, float3 P, float u1, float u2) {
     LightSample s;
     if (l.type == LIGHT_SQUARE) {                                        // squareLight.h:57-82
-        float3 lp = mk((u1 - 0.5f) * l.xs * 2.f, (u2 - 0.5f) * l.ys * 2.f, 0.f);
+        float3 lp = mk((float)(((double)u1 - 0.5) * l.xs * 2.0), (float)(((double)u2 - 0.5) * l.ys * 2.0), 0.f);
         lp = xform_point(l.m, lp);
         float3 dir = lp - P;
         float len = length(dir);
         dir = normalize(dir);
         s.dir = dir;
-        s.maxt = len - kRayBias * 10.f;
+        s.maxt = (float)((double)len - 0.005);                  // sampleLength - RAY_BIAS*10 (double)
         float d = dot(l.n, -dir);
         if (!(d > 0.f)) d = 0.f;
         s.color = l.le;
-        s.pdf = d == 0.f ? 0.f : (len * len) / (d * l.xs * l.ys * 4.f);
+        s.pdf = d == 0.f ? 0.f : (float)((double)(len * len) / ((double)(d * l.xs * l.ys) * 4.0));
         return s;
     }
     float3 wc = l.center - P;                                            // sphere (extension)
@@ -358,8 +367,8 @@ AUR_HD LightSample light_sample(const Light& l, float3 P, float u1, float u2) {
     float cosmax = sphere_cone_cos(l, P);
     float cost = (1.f - u1) + u1 * cosmax;
     float sint = sqrtf(fmaxf(0.f, 1.f - cost * cost));
-    float phi = 2.f * kPi * u2;
-    float3 dir = normalize(tangent_to_world(mk(sint * cosf(phi), sint * sinf(phi), cost), w));
+    float phi = two_pi_times(u2);
+    float3 dir = normalize(tangent_to_world(mk(sint * xcosf(phi), sint * xsinf(phi), cost), w));
     float t;
     sphere_hit(l.center, l.radius, P, dir, 0.f, &t);
     s.dir = dir;
@@ -380,8 +389,8 @@ AUR_HD float light_pdf(const Light& l, float3 o, float3 d, float mint, float* ma
         *maxt = t;
         float dd = dot(l.n, normalize(d));
         dd = dd > 0.f ? dd : (dd < 0.f ? -dd : 0.f);
-        float pdf = (t * t) / (dd * l.xs * l.ys * 4.f);
-        *maxt -= kRayBias * 10.f;
+        float pdf = (float)((double)(t * t) / ((double)(dd * l.xs * l.ys) * 4.0));
+        *maxt = (float)((double)*maxt - 0.005);
         return pdf;
     }
     float t;
@@ -401,7 +410,7 @@ struct Frame { float3 P, V, N; float su, sv; int attr; };
 AUR_HD Frame hit_frame(const ShadeScene& s, int prim, float t, float u, float v, float3 o, float3 d, bool need_uv) {
     Frame f;
     const float* n = s.corner_n + (size_t)prim * 9;
-    float w = 1.f - u - v;
+    float w = (float)(1.0 - u - v);      // 1. - u - v in double (embreeAccelerator.cpp:54)
     float3 nn = mk(w * n[0] + u * n[3] + v * n[6],
                    w * n[1] + u * n[4] + v * n[7],
                    w * n[2] + u * n[5] + v * n[8]);

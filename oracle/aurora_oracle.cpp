@@ -70,6 +70,7 @@ struct Color {
     Color operator*(const Color& c) const { return Color(r * c.r, g * c.g, b * c.b); }
     Color& operator*=(const Color& c) { r *= c.r; g *= c.g; b *= c.b; return *this; }
     Color operator*(float f) const { return Color(r * f, g * f, b * f); }
+    Color operator*(double d) const { return Color(r * d, g * d, b * d); }   // color.h:108-110
     Color& operator*=(float f) { r *= f; g *= f; b *= f; return *this; }
     Color operator/(float f) const { float d = 1 / f; return Color(r * d, g * d, b * d); }
     Color& operator/=(float f) { float d = 1 / f; r *= d; g *= d; b *= d; return *this; }
@@ -394,12 +395,12 @@ static Sample3D lambertGetSample(const BrdfState& b, const Vector& Vn, const Vec
     s.ray.direction = normalize(tangentToWorld(dir, Nn));
     s.ray.origin = Point(0, 0, 0); s.ray.mint = RAY_BIAS; s.ray.maxt = 1000000.f;
     s.pdf = M_PI_INV * 0.5;
-    s.color = b.color * (float)M_PI_INV;
+    s.color = b.color * M_PI_INV;
     return s;
 }
 static Color lambertEval(const BrdfState& b, const Vector& Ln, const Vector& Nn) {          // lambert.h:68-76
     float d = dot(Ln, Nn);
-    if (d > 0.) return b.color * (float)M_PI_INV;
+    if (d > 0.) return b.color * M_PI_INV;
     return Color(0);
 }
 
@@ -602,7 +603,7 @@ static Sample3D lightGenerateSample(const Light& l, const Point& orig, float x, 
     float cosmax = sphereConeCos(l, orig);
     float cost = (1.f - x) + x * cosmax;
     float sint = sqrtf(std::max(0.f, 1.f - cost * cost));
-    float phi = 2.f * (float)M_PI * y;
+    float phi = 2 * M_PI * y;
     Vector dir = normalize(tangentToWorld(Vector(sint * cosf(phi), sint * sinf(phi), cost), w));
     float t;
     sphereHit(l, orig, dir, 0.f, &t);
@@ -758,6 +759,8 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
         ++cnt.closest;
         if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) break;
     }
+    // firefly filter; a non-finite estimate (which would never leave the loop) is dropped
+    if (!std::isfinite(Lo.r) || !std::isfinite(Lo.g) || !std::isfinite(Lo.b)) return Color(0.f);
     while (Lo.r > FIREFLY || Lo.g > FIREFLY || Lo.b > FIREFLY) Lo *= 0.2f;
     return Lo;
 }
