@@ -106,6 +106,7 @@ SIGNATURES = {
     "aur_scene_get_params": (st, [vp, vp, vp]),
     "aur_render": (st, [vp, C.POINTER(RenderOpts), vp, C.POINTER(RenderStats)]),
     "aur_render_f64": (st, [vp, C.POINTER(RenderOpts), vp, C.POINTER(RenderStats)]),
+    "aur_render_fp64acc_noalloc": (st, [vp, C.POINTER(RenderOpts), vp, C.POINTER(RenderStats)]),
     "aur_render_batch": (st, [C.POINTER(C.c_void_p), C.POINTER(RenderOpts), C.c_uint32, C.POINTER(C.c_void_p),
                               C.POINTER(RenderStats)]),
     "aur_render_adjoint": (st, [vp, C.POINTER(RenderOpts), vp, vp, vp, C.POINTER(RenderStats)]),

@@ -223,6 +223,19 @@ AUR_API aur_status aur_render(aur_scene* scene, const aur_render_opts* opts, flo
  * doubles): the high-sample oracle images. */
 AUR_API aur_status aur_render_f64(aur_scene* scene, const aur_render_opts* opts, double* film_rgba, aur_render_stats* stats);
 
+/* The plain renderer with FP64 accumulation (the film is the FP64 sums rounded
+ * to float) that allocates no device memory. No counterpart in the reference.
+ * For callers that cannot allocate: hosts that own all device memory through
+ * their own allocator or a fixed budget. The film must be 16-byte aligned
+ * device memory (width*height*4 floats); width*height must be <= 65536. The
+ * scratch (FP64 accumulators, ray counters) is a static device array that every
+ * GPU loading the library holds until exit (2 MiB). The first call on a device
+ * looks up that array's address with the device current; make it before any
+ * stream capture. All calls share the array: calls that overlap on the GPU race
+ * and must be serialised by the caller. stats->kernel_ms is not measured (0). */
+AUR_API aur_status aur_render_fp64acc_noalloc(aur_scene* scene, const aur_render_opts* opts, float* film_device,
+                                              aur_render_stats* stats);
+
 /* Many scenes in one wavefront launch (each with its own options); films[i]
  * is width_i*height_i*4 floats. */
 AUR_API aur_status aur_render_batch(aur_scene* const* scenes, const aur_render_opts* opts, uint32_t nscenes,
