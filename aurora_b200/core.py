@@ -6,6 +6,7 @@ tensors); the library accepts both host and device pointers.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -30,10 +31,13 @@ class Context:
         check(lib().aur_ctx_create(device, C.byref(h)), "aur_ctx_create")
         self.handle = h
         self.device = device
+        self._children = weakref.WeakSet()
 
     def close(self):
         if self.handle:
-            lib().aur_ctx_destroy(self.handle)
+            for child in list(self._children):     # scenes and BVHs die before their context
+                child.close()
+            check(lib().aur_ctx_destroy(self.handle), "aur_ctx_destroy")
             self.handle = None
 
     def __del__(self):
@@ -84,6 +88,7 @@ class Bvh:
         check(lib().aur_bvh_build(ctx.handle, _ptr(verts), verts.shape[0], _ptr(tri_vidx), _ptr(attr),
                                   tri_vidx.shape[0], C.byref(opts) if opts else None, C.byref(h)), "aur_bvh_build")
         self.handle = h
+        ctx._children.add(self)
 
     def close(self):
         if self.owned and self.handle:
@@ -132,7 +137,10 @@ def render_opts(spp, max_depth, min_depth, seed, mode=_abi.RENDER_PLAIN, sample_
 def _stats(s: _abi.RenderStats) -> dict:
     return {"camera_rays": s.camera_rays, "closest_rays": s.closest_rays, "shadow_rays": s.shadow_rays,
             "paths": s.paths, "node_visits": s.node_visits, "tri_tests": s.tri_tests, "launches": s.launches,
-            "kernel_ms": s.kernel_ms}
+            "kernel_ms": s.kernel_ms, "shadow_node_visits": s.shadow_node_visits,
+            "shadow_tri_tests": s.shadow_tri_tests,
+            "stage_ms": dict(zip(("regen", "extend", "sort", "shade", "shadow"), list(s.stage_ms))),
+            "wf_config": {"pool": s.wf_pool, "block": s.wf_block, "sort": s.wf_sort}}
 
 
 class Scene:
@@ -148,6 +156,7 @@ class Scene:
             check(lib().aur_scene_create(ctx.handle, C.byref(desc), C.byref(bvh) if bvh else None, C.byref(h)),
                   "aur_scene_create")
         self.handle = h
+        ctx._children.add(self)
         w, hh, ntri, nmat, ntex = C.c_int32(), C.c_int32(), C.c_uint32(), C.c_uint32(), C.c_uint32()
         check(lib().aur_scene_info(h, C.byref(w), C.byref(hh), C.byref(ntri), C.byref(nmat), C.byref(ntex)),
               "aur_scene_info")

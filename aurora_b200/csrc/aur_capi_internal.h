@@ -2,6 +2,8 @@
 #pragma once
 #include "aurora_b200.h"
 #include "aur_kernels.h"
+#include <array>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -12,6 +14,10 @@ struct aur_ctx {
     float* kelemen = nullptr;                  // 21 tables x 2048 floats
     bool kel_ready[aur::kAlbedoRefl] = {};
     unsigned long long* counters = nullptr;    // 8 render counters
+    cudaStream_t work_stream = nullptr;        // non-blocking stream for captured work (wavefront graphs)
+    cudaEvent_t ev_order = nullptr;            // orders work_stream after `stream`
+    std::map<uint64_t, std::array<int, 3>> wf_batch_tuned;   // autotuned batch configs (pool, block, sort)
+    int live = 0;                              // BVHs and scenes created on this context and not destroyed
 };
 
 struct aur_bvh {
@@ -39,6 +45,8 @@ struct aur_scene {
     std::vector<aur::Texture> h_texs;
     uint32_t ntri = 0, nattr = 0, ntexel_floats = 0;
     aur::Camera cam{};
+    bool wf_tuned = false;                     // autotuned wavefront configuration
+    int wf_pool = 0, wf_block = 0, wf_sort = 0;
     aur::DevScene dev() const;
 };
 
@@ -52,6 +60,7 @@ int kelemen_index(float reflectance);
 aur_status bvh_options(const aur_bvh_opts* o, BvhBuildOptions* out);
 aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathParams* p);
 aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film, aur_render_stats* stats);
+void wf_release_context(aur_ctx* ctx);   // frees the wavefront engines cached for a context
 
 struct DeviceGuard {
     explicit DeviceGuard(int dev);

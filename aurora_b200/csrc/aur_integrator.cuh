@@ -29,7 +29,7 @@ struct PathParams {
     uint32_t seed;
 };
 
-struct RayCounts { uint32_t closest = 0, shadow = 0; TraceWork work; };
+struct RayCounts { uint32_t closest = 0, shadow = 0; TraceWork work, shadow_work; };
 
 // Picks the k-th light for which light_visible() holds; returns -1 if none.
 __device__ __forceinline__ int pick_visible_light(const ShadeScene& sh, float3 P, float3 N, float u, int* nvis) {
@@ -63,7 +63,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
     if (brdf.lobe == LOBE_MATTE) {
         if (cost >= 0.f && ls.pdf > 0.f) {
             ++rc.shadow;
-            if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.work))
+            if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work))
                 res += cdiv((ls.color * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
         }
     } else {
@@ -71,7 +71,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
             const float bp = brdf_pdf(brdf, ls.dir, f.V, f.N);
             if (bp > 0.f) {
                 ++rc.shadow;
-                if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.work)) {
+                if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work)) {
                     const float w = power_heuristic(ls.pdf, bp);
                     res += cdiv(((ls.color * w) * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
                 }
@@ -85,7 +85,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
             const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
             if (lp > 0.f && bs.pdf > 0.f) {
                 ++rc.shadow;
-                if (!bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.work)) {
+                if (!bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.shadow_work)) {
                     const float w = power_heuristic(bs.pdf, lp);
                     res += cdiv(((bs.color * w) * L.le) * cost, bs.pdf);
                 }

@@ -17,7 +17,8 @@ cudaError_t launch_kelemen_table(int refl_index, float* out, cudaStream_t s);
 
 // render_plain.cu — one thread per pixel, spp paths per thread.
 // counters[0..3] = camera rays, closest rays, shadow rays, paths; with count_work
-// also [4] interior-node visits and [5] triangle tests (accumulated).
+// also [4..5] interior-node visits / triangle tests of closest-hit rays and
+// [6..7] those of shadow rays (accumulated).
 cudaError_t launch_render_plain(const DevScene& sc, const PathParams& p, float4* film, double* film64,
                                 unsigned long long* counters, bool count_work, cudaStream_t s);
 

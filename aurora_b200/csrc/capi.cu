@@ -126,17 +126,30 @@ aur_status aur_ctx_create(int device, aur_ctx** out) {
     if (e != cudaSuccess) { delete c; return cuda_fail(e, "aur_ctx_create"); }
     c->own_stream = true;
     e = cudaMalloc(&c->counters, sizeof(unsigned long long) * 8);
-    if (e != cudaSuccess) { cudaStreamDestroy(c->stream); delete c; return cuda_fail(e, "aur_ctx_create"); }
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->work_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming);
+    if (e != cudaSuccess) {
+        if (c->counters) cudaFree(c->counters);
+        if (c->work_stream) cudaStreamDestroy(c->work_stream);
+        cudaStreamDestroy(c->stream);
+        delete c;
+        return cuda_fail(e, "aur_ctx_create");
+    }
     *out = c;
     return AUR_OK;
 }
 
 aur_status aur_ctx_destroy(aur_ctx* ctx) {
     if (!ctx) return AUR_OK;
+    if (ctx->live > 0)
+        return fail(AUR_ERR_INVALID_ARG, "aur_ctx_destroy: destroy the context's scenes and BVHs first");
     DeviceGuard g(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    wf_release_context(ctx);
     if (ctx->kelemen) cudaFree(ctx->kelemen);
     if (ctx->counters) cudaFree(ctx->counters);
+    if (ctx->work_stream) { cudaStreamSynchronize(ctx->work_stream); cudaStreamDestroy(ctx->work_stream); }
+    if (ctx->ev_order) cudaEventDestroy(ctx->ev_order);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return AUR_OK;
@@ -204,6 +217,7 @@ aur_status aur_bvh_build(aur_ctx* ctx, const float* verts, uint32_t nvert, const
         delete b;
         return cuda_fail(e, "aur_bvh_build");
     }
+    ++ctx->live;
     *out = b;
     return AUR_OK;
 }
@@ -211,6 +225,7 @@ aur_status aur_bvh_build(aur_ctx* ctx, const float* verts, uint32_t nvert, const
 aur_status aur_bvh_destroy(aur_bvh* b) {
     if (!b) return AUR_OK;
     if (b->owned_by_scene) return fail(AUR_ERR_INVALID_ARG, "aur_bvh_destroy: BVH belongs to a scene");
+    --b->ctx->live;
     DeviceGuard g(b->ctx->device);
     bvh_free_device(&b->bvh, b->ctx->stream);
     if (b->owns_attr && b->tri_attr) cudaFreeAsync(b->tri_attr, b->ctx->stream);

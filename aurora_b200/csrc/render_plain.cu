@@ -11,7 +11,8 @@ namespace {
 
 constexpr int kPlainBlock = 128;
 
-// counters: camera rays, closest rays, shadow rays, paths, node visits, triangle tests
+// counters: camera rays, closest rays, shadow rays, paths, then (counting variant) node visits and
+// triangle tests of closest-hit rays and of shadow rays
 template <int kN>
 __device__ __forceinline__ void add_counters(unsigned long long* counters, const uint32_t (&v_in)[kN]) {
     unsigned long long v[kN];
@@ -63,9 +64,9 @@ __global__ void __launch_bounds__(kPlainBlock) k_render_plain(DevScene sc, PathP
         }
     }
     if (kCount) {
-        const uint32_t v[6] = {pixel < npix ? (uint32_t)p.spp : 0u, rc.closest, rc.shadow, paths, rc.work.nodes,
-                               rc.work.tris};
-        add_counters<6>(counters, v);
+        const uint32_t v[8] = {pixel < npix ? (uint32_t)p.spp : 0u, rc.closest, rc.shadow, paths, rc.work.nodes,
+                               rc.work.tris, rc.shadow_work.nodes, rc.shadow_work.tris};
+        add_counters<8>(counters, v);
     } else {
         const uint32_t v[4] = {pixel < npix ? (uint32_t)p.spp : 0u, rc.closest, rc.shadow, paths};
         add_counters<4>(counters, v);

@@ -1,0 +1,936 @@
+// render_wavefront.cu — the batched (wavefront) renderer.
+//
+// Same estimator as Integrator::integrateCameraSample (Aurora/src/frontend/
+// integrator.cpp:152-300) and the plain kernel, reorganised for the GPU:
+// a pool of P path slots lives in HBM (structure of arrays) and every
+// iteration runs one bounce of every live path as separate stages:
+//
+//   regen   finished slots write their sample and take the next work item
+//           (scene, pixel, sample) from a global counter -> camera ray
+//   extend  closest hit for the extension queue (persistent warps, traversal only)
+//   sort    optional: counting sort of the hits by material type
+//   shade   emission, lobe choice, next-event rays + their contributions, BRDF
+//           continuation, throughput and roulette -> next extension queue
+//   shadow  occlusion for the next-event rays, Lo += direct * T
+//
+// Queues are compacted with warp ballots (one atomic per warp). Many scenes of
+// different resolution, spp and depth share one pool (batched launch). The
+// per-iteration kernels are captured once into a CUDA graph and replayed.
+// Every (pixel, sample) result goes to a per-sample buffer and is resolved in
+// sample order with the plain kernel's compensated sum, so both renderers
+// produce the same film for the same seed.
+#include "aur_capi_internal.h"
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <tuple>
+
+namespace aur {
+namespace {
+
+enum : uint32_t { PS_EMPTY = 0, PS_ACTIVE = 1, PS_DONE = 2 };
+enum : int { B_MISS = 0, B_MATTE = 1, B_KELEMEN = 2, B_CT = 3, B_METAL = 4, B_CONST = 5, kBuckets = 6 };
+// counters
+enum : int {
+    C_EXT0 = 0, C_EXT1 = 1, C_SHADOW = 2, C_WORK = 3, C_TOTAL = 4, C_CUR_EXT = 5, C_CUR_SHADE = 6,
+    C_CUR_SHADOW = 7, C_CUR_SORT = 8, C_BUCKET = 16, C_FILL = 24, kCounters = 32
+};
+
+struct WfScene {
+    DevScene sc;
+    PathParams p;          // spp = samples of this pass, sample_offset = first sample index of this pass
+    uint64_t key;
+    uint32_t npix, item_base, items, pad;
+    float4* samples;       // [spp_pass][npix]
+};
+
+struct WfPool {
+    float4 *ray_o, *ray_d, *tp, *lo, *hit, *sh_p, *sh_d0, *sh_d1, *sh_c0, *sh_c1, *sh_t;
+    uint4* id;
+    uint32_t* state;
+    uint32_t *q_ext0, *q_ext1, *q_sort, *q_shadow;
+    uint32_t* ctr;
+    unsigned long long* rays;   // [0] closest-hit rays, [1] shadow rays
+    const WfScene* scenes;
+    int nscenes;                // table capacity; unused entries start at item UINT32_MAX
+    uint32_t P;
+};
+
+// flags in id.w
+__device__ __forceinline__ uint32_t pack_flags(int vtx, int bounces, int kind, bool matte) {
+    return (uint32_t)vtx | ((uint32_t)bounces << 9) | ((uint32_t)kind << 18) | ((uint32_t)matte << 20);
+}
+__device__ __forceinline__ int f_vtx(uint32_t f) { return f & 511; }
+__device__ __forceinline__ int f_bounces(uint32_t f) { return (f >> 9) & 511; }
+__device__ __forceinline__ int f_kind(uint32_t f) { return (f >> 18) & 3; }
+__device__ __forceinline__ bool f_matte(uint32_t f) { return (f >> 20) & 1; }
+
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
+__device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
+
+// Warp-aggregated append: lanes with `pred` get consecutive slots of `q`.
+__device__ __forceinline__ void warp_push(bool pred, uint32_t value, uint32_t* q, uint32_t* count) {
+    const uint32_t m = __ballot_sync(0xffffffffu, pred);
+    if (!m) return;
+    uint32_t base = 0;
+    const int leader = __ffs(m) - 1;
+    if ((int)lane_id() == leader) base = atomicAdd(count, (uint32_t)__popc(m));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (pred) q[base + __popc(m & lanemask_lt())] = value;
+}
+
+// Persistent-warp fetch: returns the first index of the warp's next batch of 32.
+__device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor) {
+    uint32_t b = 0;
+    if (lane_id() == 0) b = atomicAdd(cursor, 32u);
+    return __shfl_sync(0xffffffffu, b, 0);
+}
+
+__device__ __forceinline__ int scene_of(const WfPool& w, uint32_t item) {
+    int lo = 0, hi = w.nscenes - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (w.scenes[mid].item_base <= item) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// ------------------------------------------------------------------ regen
+__global__ void k_regen(WfPool w, int in_q) {
+    uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
+    uint32_t* cin = &w.ctr[in_q ? C_EXT1 : C_EXT0];
+    const uint32_t total = w.ctr[C_TOTAL];
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x; base < w.P; base += stride) {
+        const uint32_t i = base + threadIdx.x;
+        const bool valid = i < w.P;
+        uint32_t st = valid ? w.state[i] : (uint32_t)PS_ACTIVE;
+        if (st == PS_DONE) {
+            const uint4 id = w.id[i];
+            const WfScene& S = w.scenes[id.x];
+            const float4 lo = w.lo[i];
+            const float3 L = firefly_clamp(mk(lo.x, lo.y, lo.z));
+            S.samples[(size_t)id.z * S.npix + id.y] = make_float4(L.x, L.y, L.z, lo.w);
+            st = PS_EMPTY;
+        }
+        const bool want = st == PS_EMPTY && *(volatile uint32_t*)&w.ctr[C_WORK] < total;
+        const uint32_t m = __ballot_sync(0xffffffffu, want);
+        uint32_t item = 0xffffffffu;
+        if (m) {
+            uint32_t b = 0;
+            const int leader = __ffs(m) - 1;
+            if ((int)lane_id() == leader) b = atomicAdd(&w.ctr[C_WORK], (uint32_t)__popc(m));
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (want) item = b + __popc(m & lanemask_lt());
+        }
+        const bool start = want && item < total;
+        if (start) {
+            const int s = scene_of(w, item);
+            const WfScene& S = w.scenes[s];
+            const uint32_t local = item - S.item_base;
+            const uint32_t pixel = local % S.npix, sl = local / S.npix;
+            PathRng rng;
+            rng.key = S.key;
+            rng.base = path_base(pixel, (uint32_t)S.p.sample_offset + sl);
+            const RayF r = camera_ray(S.sc.cam, (int)(pixel % (uint32_t)S.sc.cam.w), (int)(pixel / (uint32_t)S.sc.cam.w),
+                                      rng.u(kDimCamera), rng.u(kDimCamera + 1));
+            w.ray_o[i] = make_float4(r.o.x, r.o.y, r.o.z, r.mint);
+            w.ray_d[i] = make_float4(r.d.x, r.d.y, r.d.z, r.maxt);
+            w.tp[i] = make_float4(1.f, 1.f, 1.f, 1.f);
+            w.lo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+            w.id[i] = make_uint4((uint32_t)s, pixel, sl, pack_flags(0, 0, RAY_CAMERA, false));
+            st = PS_ACTIVE;
+        }
+        warp_push(start, i, qin, cin);
+        if (valid) w.state[i] = st;
+    }
+}
+
+// ------------------------------------------------------------------ extend
+template <bool kSort>
+__global__ void k_extend(WfPool w, int in_q) {
+    const uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
+    const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
+    // Outputs of the later stages start empty. Only counters that no block of
+    // this kernel touches are reset here; the bucket counters this kernel
+    // increments were reset by the previous shade (or the pass start).
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.ctr[in_q ? C_EXT0 : C_EXT1] = 0;
+        w.ctr[C_SHADOW] = 0;
+        w.ctr[C_CUR_SHADE] = 0;
+        w.ctr[C_CUR_SHADOW] = 0;
+        w.ctr[C_CUR_SORT] = 0;
+        w.rays[0] += n;
+    }
+    while (true) {
+        const uint32_t b = warp_fetch(&w.ctr[C_CUR_EXT]);
+        if (b >= n) break;
+        const uint32_t k = b + lane_id();
+        int bucket = -1;
+        if (k < n) {
+            const uint32_t slot = qin[k];
+            const float4 o = w.ray_o[slot], d = w.ray_d[slot];
+            const WfScene& S = w.scenes[w.id[slot].x];
+            Hit h;
+            TraceWork work;
+            const bool hit = bvh_closest(S.sc.nodes, S.sc.tris, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, d.w, &h, work);
+            w.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : -1));
+            if (kSort) {
+                bucket = B_MISS;
+                if (hit) {
+                    const int mt = S.sc.sh.mats[S.sc.sh.attrs[S.sc.sh.tri_attr[h.prim]].material].type;
+                    bucket = mt == MAT_MATTE ? B_MATTE : mt == MAT_KELEMEN ? B_KELEMEN : mt == MAT_COOKTORRANCE ? B_CT
+                           : mt == MAT_METAL ? B_METAL : B_CONST;
+                }
+            }
+        }
+        if (kSort) {
+            // per-bucket counts, one atomic per (warp, bucket)
+            const uint32_t active = __ballot_sync(0xffffffffu, bucket >= 0);
+            if (bucket >= 0) {
+                const uint32_t peers = __match_any_sync(active, bucket);
+                if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&w.ctr[C_BUCKET + bucket], (uint32_t)__popc(peers));
+            }
+        }
+    }
+}
+
+// counting-sort scatter of the extension queue into q_sort, grouped by bucket
+__global__ void k_sort_scatter(WfPool w, int in_q) {
+    const uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
+    const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
+    __shared__ uint32_t s_ofs[kBuckets];
+    if (threadIdx.x == 0) {
+        uint32_t a = 0;
+        for (int b = 0; b < kBuckets; ++b) { s_ofs[b] = a; a += w.ctr[C_BUCKET + b]; }
+    }
+    __syncthreads();
+    while (true) {
+        const uint32_t b = warp_fetch(&w.ctr[C_CUR_SORT]);
+        if (b >= n) break;
+        const uint32_t k = b + lane_id();
+        int bucket = -1;
+        uint32_t slot = 0;
+        if (k < n) {
+            slot = qin[k];
+            const float4 h = w.hit[slot];
+            const int prim = __float_as_int(h.w);
+            bucket = B_MISS;
+            if (prim >= 0) {
+                const WfScene& S = w.scenes[w.id[slot].x];
+                const int mt = S.sc.sh.mats[S.sc.sh.attrs[S.sc.sh.tri_attr[prim]].material].type;
+                bucket = mt == MAT_MATTE ? B_MATTE : mt == MAT_KELEMEN ? B_KELEMEN : mt == MAT_COOKTORRANCE ? B_CT
+                       : mt == MAT_METAL ? B_METAL : B_CONST;
+            }
+        }
+        const uint32_t active = __ballot_sync(0xffffffffu, bucket >= 0);
+        if (bucket >= 0) {
+            const uint32_t peers = __match_any_sync(active, bucket);
+            const int leader = __ffs(peers) - 1;
+            uint32_t base = 0;
+            if ((int)lane_id() == leader) base = atomicAdd(&w.ctr[C_FILL + bucket], (uint32_t)__popc(peers));
+            base = __shfl_sync(peers, base, leader);
+            w.q_sort[s_ofs[bucket] + base + __popc(peers & lanemask_lt())] = slot;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ shade
+__global__ void k_shade(WfPool w, int in_q, int sorted) {
+    const uint32_t* qin = sorted ? w.q_sort : (in_q ? w.q_ext1 : w.q_ext0);
+    const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
+    uint32_t* qout = in_q ? w.q_ext0 : w.q_ext1;
+    uint32_t* cout = &w.ctr[in_q ? C_EXT0 : C_EXT1];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {   // extend and scatter are finished: reset their counters
+        w.ctr[C_CUR_EXT] = 0;
+        for (int k = 0; k < kBuckets; ++k) { w.ctr[C_BUCKET + k] = 0; w.ctr[C_FILL + k] = 0; }
+    }
+    while (true) {
+        const uint32_t b = warp_fetch(&w.ctr[C_CUR_SHADE]);
+        if (b >= n) break;
+        const uint32_t k = b + lane_id();
+        bool push_ext = false, push_sh = false;
+        uint32_t slot = 0;
+        if (k < n) {
+            slot = qin[k];
+            const float4 hh = w.hit[slot];
+            const int prim = __float_as_int(hh.w);
+            float4 lo = w.lo[slot];
+            if (prim < 0) {
+                w.state[slot] = PS_DONE;
+            } else {
+                const uint4 id = w.id[slot];
+                const WfScene& S = w.scenes[id.x];
+                const DevScene& sc = S.sc;
+                const uint32_t flags = id.w;
+                const int vtx = f_vtx(flags);
+                int kind = f_kind(flags);
+                bool matte = f_matte(flags);
+                int bounces = f_bounces(flags);
+                PathRng rng;
+                rng.key = S.key;
+                rng.base = path_base(id.y, (uint32_t)S.p.sample_offset + id.z);
+                const float4 ro = w.ray_o[slot], rd = w.ray_d[slot];
+                float4 tpv = w.tp[slot];
+                float3 T = mk(tpv.x, tpv.y, tpv.z);
+                float cont = tpv.w;
+                float3 Lo = mk(lo.x, lo.y, lo.z);
+                if (vtx == 0) lo.w = 1.f;   // camera ray hit: alpha
+                const Frame f = hit_frame(sc.sh, prim, hh.x, hh.y, hh.z, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), true);
+                const Attr at = sc.sh.attrs[f.attr];
+                if (kind == RAY_DIFFUSE) matte = true;
+                if (kind == RAY_CAMERA) Lo += T * at.emission;
+                const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
+                                           rng.u(vertex_dim(vtx, kDimLobe)));
+                // next-event estimation: rays and their unoccluded contributions
+                if (brdf.lobe == LOBE_MATTE || brdf.lobe == LOBE_SPEC) {
+                    int nvis;
+                    const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
+                    if (li >= 0) {
+                        const Light L = sc.sh.lights[li];
+                        const LightSample ls = light_sample(L, f.P, rng.u(vertex_dim(vtx, kDimLightSample)),
+                                                            rng.u(vertex_dim(vtx, kDimLightSample + 1)));
+                        float cost = dot(f.N, ls.dir);
+                        float3 c0 = mk(0.f, 0.f, 0.f), c1 = c0;
+                        float3 d0 = ls.dir, d1 = ls.dir;
+                        float m0 = ls.maxt, m1 = 0.f;
+                        bool r0 = false, r1 = false;
+                        if (brdf.lobe == LOBE_MATTE) {
+                            if (cost >= 0.f && ls.pdf > 0.f) {
+                                r0 = true;
+                                c0 = cdiv((ls.color * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
+                            }
+                        } else {
+                            if (cost > 0.f && ls.pdf > 0.f) {
+                                const float bp = brdf_pdf(brdf, ls.dir, f.V, f.N);
+                                if (bp > 0.f) {
+                                    r0 = true;
+                                    const float wgt = power_heuristic(ls.pdf, bp);
+                                    c0 = cdiv(((ls.color * wgt) * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
+                                }
+                            }
+                            const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimMisBrdf)),
+                                                              rng.u(vertex_dim(vtx, kDimMisBrdf + 1)));
+                            cost = dot(f.N, bs.dir);
+                            if (cost > 0.f) {
+                                float maxt = bs.maxt;
+                                const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
+                                if (lp > 0.f && bs.pdf > 0.f) {
+                                    r1 = true;
+                                    d1 = bs.dir;
+                                    m1 = maxt;
+                                    const float wgt = power_heuristic(bs.pdf, lp);
+                                    c1 = cdiv(((bs.color * wgt) * L.le) * cost, bs.pdf);
+                                }
+                            }
+                        }
+                        if (r0 || r1) {
+                            w.sh_p[slot] = make_float4(f.P.x, f.P.y, f.P.z, (float)nvis);
+                            w.sh_d0[slot] = make_float4(d0.x, d0.y, d0.z, m0);
+                            w.sh_d1[slot] = make_float4(d1.x, d1.y, d1.z, m1);
+                            w.sh_c0[slot] = make_float4(c0.x, c0.y, c0.z, r0 ? 1.f : 0.f);
+                            w.sh_c1[slot] = make_float4(c1.x, c1.y, c1.z, r1 ? 1.f : 0.f);
+                            w.sh_t[slot] = make_float4(T.x, T.y, T.z, 0.f);
+                            push_sh = true;
+                        }
+                    }
+                }
+                // continuation (integrator.cpp:208-261)
+                bool alive = false;
+                const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
+                                                  rng.u(vertex_dim(vtx, kDimBrdf + 1)));
+                if (bs.pdf > 0.f) {
+                    const float cosl = dot(f.N, bs.dir);
+                    T *= cdiv(bs.color * cosl, bs.pdf);
+                    if (bounces > S.p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
+                    if (!is_black(T)) {
+                        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
+                        bool rr_ok = true;
+                        if (bounces > S.p.min_depth) {
+                            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) rr_ok = false;
+                            else T = cdiv(T, cont);
+                        }
+                        if (rr_ok) {
+                            ++bounces;
+                            if (vtx + 1 < S.p.max_depth) {
+                                alive = true;
+                                w.ray_o[slot] = make_float4(f.P.x, f.P.y, f.P.z, kRayBias);
+                                w.ray_d[slot] = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.maxt);
+                                w.tp[slot] = make_float4(T.x, T.y, T.z, cont);
+                                w.id[slot].w = pack_flags(vtx + 1, bounces, kind, matte);
+                            }
+                        }
+                    }
+                }
+                lo = make_float4(Lo.x, Lo.y, Lo.z, lo.w);
+                w.state[slot] = alive ? PS_ACTIVE : PS_DONE;
+                push_ext = alive;
+            }
+            w.lo[slot] = lo;
+        }
+        warp_push(push_ext, slot, qout, cout);
+        warp_push(push_sh, slot, w.q_shadow, &w.ctr[C_SHADOW]);
+    }
+}
+
+// ------------------------------------------------------------------ shadow
+__global__ void k_shadow(WfPool w) {
+    const uint32_t n = w.ctr[C_SHADOW];
+    uint32_t nrays = 0;
+    while (true) {
+        const uint32_t b = warp_fetch(&w.ctr[C_CUR_SHADOW]);
+        if (b >= n) break;
+        const uint32_t k = b + lane_id();
+        if (k < n) {
+            const uint32_t slot = w.q_shadow[k];
+            const WfScene& S = w.scenes[w.id[slot].x];
+            const float4 p = w.sh_p[slot], c0 = w.sh_c0[slot], c1 = w.sh_c1[slot];
+            const float3 P = mk(p.x, p.y, p.z);
+            TraceWork work;
+            float3 res = mk(0.f, 0.f, 0.f);
+            nrays += (c0.w != 0.f) + (c1.w != 0.f);
+            if (c0.w != 0.f) {
+                const float4 d = w.sh_d0[slot];
+                if (!bvh_occluded(S.sc.nodes, S.sc.tris, P, mk(d.x, d.y, d.z), kRayBias, d.w, work))
+                    res += mk(c0.x, c0.y, c0.z);
+            }
+            if (c1.w != 0.f) {
+                const float4 d = w.sh_d1[slot];
+                if (!bvh_occluded(S.sc.nodes, S.sc.tris, P, mk(d.x, d.y, d.z), kRayBias, d.w, work))
+                    res += mk(c1.x, c1.y, c1.z);
+            }
+            const float4 t = w.sh_t[slot];
+            float4 lo = w.lo[slot];
+            const float3 add = (res * p.w) * mk(t.x, t.y, t.z);
+            lo.x += add.x; lo.y += add.y; lo.z += add.z;
+            w.lo[slot] = lo;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) nrays += __shfl_xor_sync(0xffffffffu, nrays, o);
+    if (lane_id() == 0 && nrays) atomicAdd(&w.rays[1], (unsigned long long)nrays);
+}
+
+// ------------------------------------------------------------------ resolve
+// Adds this pass's samples of every pixel, in sample order, to the per-pixel
+// compensated sums (the plain kernel's accumulation order).
+__global__ void k_resolve(const WfScene* scenes, int s, float4* acc_s, float4* acc_c) {
+    const WfScene& S = scenes[s];
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= S.npix) return;
+    const float4 a = acc_s[pixel], c = acc_c[pixel];
+    Kahan3 k;
+    k.s = mk(a.x, a.y, a.z);
+    k.c = mk(c.x, c.y, c.z);
+    float alpha = a.w;
+    for (int j = 0; j < S.p.spp; ++j) {
+        const float4 v = S.samples[(size_t)j * S.npix + pixel];
+        k.add(mk(v.x, v.y, v.z));
+        alpha += v.w;
+    }
+    acc_s[pixel] = make_float4(k.s.x, k.s.y, k.s.z, alpha);
+    acc_c[pixel] = make_float4(k.c.x, k.c.y, k.c.z, 0.f);
+}
+
+__global__ void k_finish(const float4* acc_s, const float4* acc_c, uint32_t npix, int spp, float4* film) {
+    const uint32_t pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    if (pixel >= npix) return;
+    const float inv = 1.f / (float)spp;
+    const float4 a = acc_s[pixel], c = acc_c[pixel];
+    const float3 t = mk(a.x, a.y, a.z) + mk(c.x, c.y, c.z);
+    film[pixel] = make_float4(t.x * inv, t.y * inv, t.z * inv, a.w * inv);
+}
+
+}  // namespace
+
+struct WfConfig {
+    uint32_t pool = 1u << 21;
+    int block = 128;
+    int sort = 1;
+};
+
+// ------------------------------------------------------------------ host driver
+struct WfRun {
+    // one wavefront engine: pool buffers + a captured graph of kItersPerGraph iterations
+    WfConfig cfg;
+    WfPool w{};
+    void* mem = nullptr;
+    WfScene* d_scenes = nullptr;
+    int cap_scenes = 0;
+    float4* samples = nullptr;                 // per-sample buffer, grown on demand
+    size_t samples_bytes = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t stream = nullptr;
+    int grid_regen = 0, grid_ext = 0, grid_shade = 0, grid_shadow = 0, grid_sort = 0;
+    uint32_t* h_ctr = nullptr;   // pinned
+    static constexpr int kItersPerGraph = 8;
+    static constexpr int kStages = 5;          // regen, extend, sort, shade, shadow
+    cudaEvent_t ev[kItersPerGraph * kStages + 1] = {};
+    int launches_per_graph = 0;
+    double stage_ms[kStages] = {0, 0, 0, 0, 0};
+
+    cudaError_t init(const WfConfig& c, int nscenes, cudaStream_t s) {
+        cfg = c;
+        stream = s;
+        const size_t P = c.pool;
+        const size_t bytes = P * (11 * sizeof(float4) + sizeof(uint4) + 5 * sizeof(uint32_t)) + 18 * 256 +
+                             kCounters * sizeof(uint32_t) + 2 * sizeof(unsigned long long);
+        cudaError_t e = cudaMalloc(&mem, bytes);
+        if (e != cudaSuccess) return e;
+        char* p = (char*)mem;
+        auto take = [&](size_t n) { char* r = p; p += (n + 255) & ~(size_t)255; return (void*)r; };
+        float4** f4s[] = {&w.ray_o, &w.ray_d, &w.tp, &w.lo, &w.hit, &w.sh_p, &w.sh_d0, &w.sh_d1, &w.sh_c0, &w.sh_c1, &w.sh_t};
+        for (float4** q : f4s) *q = (float4*)take(P * sizeof(float4));
+        w.id = (uint4*)take(P * sizeof(uint4));
+        w.state = (uint32_t*)take(P * 4);
+        w.q_ext0 = (uint32_t*)take(P * 4);
+        w.q_ext1 = (uint32_t*)take(P * 4);
+        w.q_sort = (uint32_t*)take(P * 4);
+        w.q_shadow = (uint32_t*)take(P * 4);
+        w.ctr = (uint32_t*)take(kCounters * 4);
+        w.rays = (unsigned long long*)take(2 * sizeof(unsigned long long));
+        if ((size_t)(p - (char*)mem) > bytes) return cudaErrorMemoryAllocation;
+        cap_scenes = std::max(nscenes, 64);
+        e = cudaMalloc(&d_scenes, sizeof(WfScene) * cap_scenes);
+        if (e != cudaSuccess) return e;
+        w.scenes = d_scenes;
+        w.nscenes = cap_scenes;
+        w.P = (uint32_t)P;
+        e = cudaMallocHost(&h_ctr, kCounters * 4);
+        if (e != cudaSuccess) return e;
+        for (auto& x : ev) if ((e = cudaEventCreate(&x)) != cudaSuccess) return e;
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        auto persist = [&](const void* fn) {
+            int nb = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, c.block, 0);
+            return std::max(1, nb) * sms;
+        };
+        grid_ext = persist(c.sort ? (const void*)k_extend<true> : (const void*)k_extend<false>);
+        grid_shade = persist((const void*)k_shade);
+        grid_shadow = persist((const void*)k_shadow);
+        grid_sort = persist((const void*)k_sort_scatter);
+        grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 16);
+        return cudaSuccess;
+    }
+
+    // One iteration; an event after every stage so the graph reports per-stage device time.
+    void enqueue_iteration(int in_q, int it) {
+        // inside stream capture only an "external" record becomes an event-record node
+        cudaEvent_t* e = &ev[it * kStages + 1];
+        k_regen<<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
+        cudaEventRecordWithFlags(e[0], stream, cudaEventRecordExternal);
+        if (cfg.sort) k_extend<true><<<grid_ext, cfg.block, 0, stream>>>(w, in_q);
+        else k_extend<false><<<grid_ext, cfg.block, 0, stream>>>(w, in_q);
+        cudaEventRecordWithFlags(e[1], stream, cudaEventRecordExternal);
+        if (cfg.sort) k_sort_scatter<<<grid_sort, cfg.block, 0, stream>>>(w, in_q);
+        cudaEventRecordWithFlags(e[2], stream, cudaEventRecordExternal);
+        k_shade<<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
+        cudaEventRecordWithFlags(e[3], stream, cudaEventRecordExternal);
+        k_shadow<<<grid_shadow, cfg.block, 0, stream>>>(w);
+        cudaEventRecordWithFlags(e[4], stream, cudaEventRecordExternal);
+    }
+
+    cudaError_t build_graph() {
+        cudaGraph_t g;
+        cudaError_t e = cudaStreamBeginCapture(stream, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return e;
+        cudaEventRecordWithFlags(ev[0], stream, cudaEventRecordExternal);
+        for (int it = 0; it < kItersPerGraph; ++it) enqueue_iteration(it & 1, it);
+        e = cudaStreamEndCapture(stream, &g);
+        if (e != cudaSuccess) return e;
+        e = cudaGraphInstantiate(&exec, g, 0);
+        cudaGraphDestroy(g);
+        launches_per_graph = kItersPerGraph * (cfg.sort ? 5 : 4);
+        return e;
+    }
+
+    // Runs one pass over `total` work items of the uploaded scene table.
+    cudaError_t run_pass(uint32_t total, uint64_t* launches) {
+        cudaError_t e = cudaMemsetAsync(w.ctr, 0, kCounters * 4, stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(w.state, 0, (size_t)w.P * 4, stream);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&w.ctr[C_TOTAL], &total, 4, cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return e;
+        if (!exec && (e = build_graph()) != cudaSuccess) return e;
+        // Bound on graph launches: each launch advances every live path by 8 bounces
+        // and refills the pool, so a pass needs about total / P * depth / 8 launches.
+        const uint64_t max_launches = (uint64_t)total * 64ull / ((uint64_t)w.P) + 4096ull;
+        for (uint64_t it = 0; it < max_launches; ++it) {
+            e = cudaGraphLaunch(exec, stream);
+            if (e != cudaSuccess) return e;
+            *launches += launches_per_graph;
+            e = cudaMemcpyAsync(h_ctr, w.ctr, 8 * 4, cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e != cudaSuccess) return e;
+            for (int k = 0; k < kItersPerGraph * kStages; ++k) {
+                float ms = 0.f;
+                if (cudaEventElapsedTime(&ms, ev[k], ev[k + 1]) == cudaSuccess) stage_ms[k % kStages] += ms;
+                else cudaGetLastError();   // timing is informational; never leave a stale error behind
+            }
+            if (h_ctr[C_WORK] >= total && h_ctr[C_EXT0] == 0) {
+                k_regen<<<grid_regen, cfg.block, 0, stream>>>(w, 0);   // writes the last finished samples
+                *launches += 1;
+                return cudaGetLastError();
+            }
+        }
+        return cudaErrorLaunchTimeout;
+    }
+
+    cudaError_t ensure_samples(size_t bytes) {
+        if (bytes <= samples_bytes) return cudaSuccess;
+        if (samples) cudaFree(samples);
+        samples = nullptr;
+        samples_bytes = 0;
+        cudaError_t e = cudaMalloc(&samples, bytes);
+        if (e == cudaSuccess) samples_bytes = bytes;
+        return e;
+    }
+
+    void release() {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (mem) cudaFree(mem);
+        if (d_scenes) cudaFree(d_scenes);
+        if (samples) cudaFree(samples);
+        samples = nullptr;
+        samples_bytes = 0;
+        if (h_ctr) cudaFreeHost(h_ctr);
+        for (auto& x : ev) if (x) cudaEventDestroy(x);
+        exec = nullptr; mem = nullptr; d_scenes = nullptr; h_ctr = nullptr;
+        for (auto& x : ev) x = nullptr;
+    }
+};
+
+struct BatchItem {
+    aur_scene* scene;
+    PathParams p;
+    uint32_t npix;
+    float4* acc_s;
+    float4* acc_c;
+};
+
+// Fills the scene table of one pass: samples [s0, s0 + chunk) of every scene.
+static uint32_t fill_table(std::vector<BatchItem>& items, int s0, int chunk, float4* samples, std::vector<WfScene>& tab,
+                           int capacity) {
+    uint32_t base = 0;
+    size_t off = 0;
+    tab.assign(capacity, WfScene());
+    for (int i = (int)items.size(); i < capacity; ++i) tab[i].item_base = 0xffffffffu;   // never selected
+    for (size_t i = 0; i < items.size(); ++i) {
+        WfScene& t = tab[i];
+        memset(&t, 0, sizeof(t));
+        t.sc = items[i].scene->dev();
+        t.p = items[i].p;
+        const int pass_spp = std::max(0, std::min(chunk, items[i].p.spp - s0));
+        t.p.spp = pass_spp;
+        t.p.sample_offset = items[i].p.sample_offset + s0;
+        t.key = seed_key(items[i].p.seed);
+        t.npix = items[i].npix;
+        t.item_base = base;
+        t.items = t.npix * (uint32_t)pass_spp;
+        t.samples = samples + off;
+        base += t.items;
+        off += (size_t)t.npix * chunk;
+    }
+    return base;
+}
+
+// Autotuner: times every candidate (pool size x block size x material sort) on the
+// same probe — the first `limit` work items of the real workload — and keeps the
+// fastest. Returns the chosen configuration.
+static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig* best_out) {
+    cudaStream_t s = ctx->work_stream;
+    size_t per_sample = 0;
+    uint64_t total = 0;
+    for (auto& it : items) { per_sample += (size_t)it.npix * sizeof(float4); total += (uint64_t)it.npix * it.p.spp; }
+    const uint32_t limit = (uint32_t)std::min<uint64_t>(total, 1ull << 24);
+    int chunk = 1;   // samples buffer large enough for the probe's first `limit` items
+    {
+        uint32_t covered = 0;
+        while (covered < limit) { covered = 0; for (auto& it : items) covered += it.npix * std::min(chunk, it.p.spp); ++chunk; }
+    }
+    float4* samples = nullptr;
+    cudaError_t e = cudaMallocAsync(&samples, per_sample * chunk, s);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront autotune");
+    std::vector<WfScene> tab;
+    fill_table(items, 0, chunk, samples, tab, std::max((int)items.size(), 64));
+    const uint32_t pools[3] = {1u << 20, 1u << 21, 1u << 22};
+    const int blocks[2] = {128, 256};
+    double best = -1.0;
+    WfConfig bestc;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    bool warmed = false;
+    for (int pi = 0; pi < 3 && e == cudaSuccess; ++pi)
+        for (int bi = 0; bi < 2 && e == cudaSuccess; ++bi)
+            for (int so = 0; so < 2 && e == cudaSuccess; ++so) {
+                WfConfig c;
+                c.pool = pools[pi];
+                c.block = blocks[bi];
+                c.sort = so;
+                WfRun run;
+                e = run.init(c, (int)items.size(), s);
+                if (e == cudaSuccess)
+                    e = cudaMemcpyAsync(run.d_scenes, tab.data(), sizeof(WfScene) * tab.size(), cudaMemcpyHostToDevice, s);
+                uint64_t l = 0;
+                if (e == cudaSuccess && !warmed) { e = run.run_pass(std::min<uint32_t>(limit, 1u << 20), &l); warmed = true; }
+                cudaEventRecord(e0, s);
+                if (e == cudaSuccess) e = run.run_pass(limit, &l);
+                cudaEventRecord(e1, s);
+                if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+                float ms = 0.f;
+                if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+                run.release();
+                if (e == cudaErrorMemoryAllocation) { cudaGetLastError(); e = cudaSuccess; continue; }
+                const double rate = ms > 0.f ? limit / ms : 0.0;
+                if (e == cudaSuccess && rate > best) { best = rate; bestc = c; }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFreeAsync(samples, s);
+    cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront autotune");
+    if (best < 0) return fail(AUR_ERR_OOM, "wavefront autotune: no configuration fits in device memory");
+    *best_out = bestc;
+    return AUR_OK;
+}
+
+// Engines (pool buffers, captured graph, events, sample buffer) are cached per
+// (context, configuration) and reused by later calls; aur_ctx_destroy releases them.
+static std::mutex g_engine_mutex;
+static std::map<std::tuple<aur_ctx*, uint32_t, int, int>, std::unique_ptr<WfRun>> g_engines;
+
+static WfRun* engine_for(aur_ctx* ctx, const WfConfig& cfg, int nscenes, cudaError_t* err) {
+    std::lock_guard<std::mutex> lock(g_engine_mutex);
+    const auto key = std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort);
+    auto it = g_engines.find(key);
+    if (it != g_engines.end() && it->second->cap_scenes >= nscenes) return it->second.get();
+    if (it != g_engines.end()) { it->second->release(); g_engines.erase(it); }
+    std::unique_ptr<WfRun> r(new WfRun());
+    *err = r->init(cfg, nscenes, ctx->work_stream);
+    if (*err != cudaSuccess) { r->release(); return nullptr; }
+    WfRun* raw = r.get();
+    g_engines.emplace(key, std::move(r));
+    return raw;
+}
+
+static void wf_drop_engine(aur_ctx* ctx, const WfConfig& cfg) {
+    std::lock_guard<std::mutex> lock(g_engine_mutex);
+    auto it = g_engines.find(std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort));
+    if (it != g_engines.end()) { it->second->release(); g_engines.erase(it); }
+}
+
+void wf_release_context(aur_ctx* ctx) {
+    std::lock_guard<std::mutex> lock(g_engine_mutex);
+    for (auto it = g_engines.begin(); it != g_engines.end();) {
+        if (std::get<0>(it->first) == ctx) { it->second->release(); it = g_engines.erase(it); }
+        else ++it;
+    }
+}
+
+// Renders a batch of scenes with the wavefront engine. films[i]: device float4[npix].
+static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, const WfConfig& cfg,
+                                  std::vector<float4*>& films, aur_render_stats* stats, float* kernel_ms) {
+    const int n = (int)items.size();
+    // The engine runs on the context's own non-blocking stream (graph capture is not
+    // allowed on the legacy default stream), ordered after the caller's stream.
+    cudaStream_t s = ctx->work_stream;
+    cudaEventRecord(ctx->ev_order, ctx->stream);
+    cudaStreamWaitEvent(s, ctx->ev_order, 0);
+    cudaError_t e = cudaSuccess;
+    WfRun* engine = engine_for(ctx, cfg, n, &e);
+    if (!engine) return cuda_fail(e, "wavefront: pool allocation");
+    WfRun& run = *engine;
+    // sample-buffer budget: passes over the spp range when all samples do not fit
+    const size_t budget = (size_t)3 << 30;
+    size_t per_sample = 0;
+    int max_spp = 0;
+    for (auto& it : items) { per_sample += (size_t)it.npix * sizeof(float4); max_spp = std::max(max_spp, it.p.spp); }
+    const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)max_spp, budget / std::max<size_t>(per_sample, 1)));
+    e = run.ensure_samples(per_sample * chunk);
+    float4* samples = run.samples;
+    for (auto& it : items) {
+        if (e == cudaSuccess) e = cudaMemsetAsync(it.acc_s, 0, sizeof(float4) * it.npix, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(it.acc_c, 0, sizeof(float4) * it.npix, s);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(run.w.rays, 0, 2 * sizeof(unsigned long long), s);
+    for (double& x : run.stage_ms) x = 0.0;
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront: sample buffers");
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    uint64_t launches = 0;
+    std::vector<WfScene> tab;
+    for (int s0 = 0; s0 < max_spp && e == cudaSuccess; s0 += chunk) {
+        const uint32_t total = fill_table(items, s0, chunk, samples, tab, run.cap_scenes);
+        e = cudaMemcpyAsync(run.d_scenes, tab.data(), sizeof(WfScene) * run.cap_scenes, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess) e = run.run_pass(total, &launches);
+        for (int i = 0; i < n && e == cudaSuccess; ++i) {
+            if (tab[i].p.spp == 0) continue;
+            k_resolve<<<(items[i].npix + 255) / 256, 256, 0, s>>>(run.d_scenes, i, items[i].acc_s, items[i].acc_c);
+            ++launches;
+            e = cudaGetLastError();
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // the scene table is rewritten next pass
+    }
+    for (int i = 0; i < n && e == cudaSuccess; ++i) {
+        k_finish<<<(items[i].npix + 255) / 256, 256, 0, s>>>(items[i].acc_s, items[i].acc_c, items[i].npix,
+                                                             items[i].p.spp, films[i]);
+        ++launches;
+        e = cudaGetLastError();
+    }
+    cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    unsigned long long rays[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(rays, run.w.rays, sizeof(rays), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    cudaEventRecord(ctx->ev_order, s);              // the caller's stream continues after this work
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_order, 0);
+    double stage[WfRun::kStages];
+    for (int k = 0; k < WfRun::kStages; ++k) stage[k] = run.stage_ms[k];
+    if (e != cudaSuccess) wf_drop_engine(ctx, cfg);   // never reuse an engine left in an unknown state
+    if (e == cudaErrorLaunchTimeout) return fail(AUR_ERR_TIMEOUT, "wavefront: the path pool did not drain");
+    if (e != cudaSuccess) return cuda_fail(e, "wavefront");
+    *kernel_ms = ms;
+    if (stats) {
+        uint64_t paths = 0;
+        for (auto& it : items) paths += (uint64_t)it.npix * it.p.spp;
+        stats->paths = paths;
+        stats->camera_rays = paths;
+        stats->closest_rays = rays[0];
+        stats->shadow_rays = rays[1];
+        stats->launches = launches;
+        stats->kernel_ms = ms;
+        for (int k = 0; k < WfRun::kStages; ++k) stats->stage_ms[k] = stage[k];
+        stats->wf_pool = (int32_t)cfg.pool;
+        stats->wf_block = cfg.block;
+        stats->wf_sort = cfg.sort;
+    }
+    return AUR_OK;
+}
+
+static bool wants_tuning(const aur_render_opts* o) { return o->wf_pool == 0 && o->wf_block == 0 && o->wf_sort < 0; }
+
+static WfConfig config_from(const aur_render_opts* o, const WfConfig& base) {
+    WfConfig c = base;
+    if (o->wf_pool > 0) c.pool = (uint32_t)o->wf_pool;
+    if (o->wf_block > 0) c.block = o->wf_block;
+    if (o->wf_sort >= 0) c.sort = o->wf_sort;
+    return c;
+}
+
+static aur_status check_config(const WfConfig& c) {
+    if (c.pool < 1024 || c.pool > (1u << 26) || (c.pool & 31))
+        return fail(AUR_ERR_INVALID_ARG, "wavefront: pool must be a multiple of 32 in [1024, 2^26]");
+    if (c.block != 64 && c.block != 128 && c.block != 256 && c.block != 512)
+        return fail(AUR_ERR_INVALID_ARG, "wavefront: block must be 64, 128, 256 or 512");
+    return AUR_OK;
+}
+
+aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film, aur_render_stats* stats) {
+    if (!sc || !o || !film) return fail(AUR_ERR_INVALID_ARG, "aur_render: NULL argument");
+    PathParams p;
+    aur_status st = render_options(sc, o, &p);
+    if (st != AUR_OK) return st;
+    if (o->count_work) return fail(AUR_ERR_UNSUPPORTED, "aur_render: count_work is implemented by the plain renderer");
+    WfConfig cfg = config_from(o, WfConfig());
+    if ((st = check_config(cfg)) != AUR_OK) return st;
+    DeviceGuard g(sc->ctx->device);
+    cudaStream_t s = sc->ctx->stream;
+    const uint32_t npix = (uint32_t)sc->cam.w * sc->cam.h;
+    if ((uint64_t)npix * o->spp >= (1ull << 31)) return fail(AUR_ERR_INVALID_ARG, "aur_render: more than 2^31 paths");
+    DevOut fo;
+    cudaError_t e = fo.init(film, sizeof(float4) * npix, 16, s);
+    float4 *acc = nullptr;
+    if (e == cudaSuccess) e = cudaMallocAsync(&acc, sizeof(float4) * 2 * npix, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // buffers allocated on the caller's stream
+    if (e != cudaSuccess) return cuda_fail(e, "aur_render(wavefront)");
+    std::vector<BatchItem> items(1);
+    items[0] = {sc, p, npix, acc, acc + npix};
+    if (wants_tuning(o)) {
+        if (!sc->wf_tuned) {
+            WfConfig t;
+            if ((st = autotune(sc->ctx, items, &t)) != AUR_OK) { cudaFreeAsync(acc, s); return st; }
+            sc->wf_pool = t.pool; sc->wf_block = t.block; sc->wf_sort = t.sort; sc->wf_tuned = true;
+        }
+        cfg.pool = sc->wf_pool; cfg.block = sc->wf_block; cfg.sort = sc->wf_sort;
+    }
+    std::vector<float4*> films = {(float4*)fo.ptr};
+    float ms = 0.f;
+    st = wavefront_batch(sc->ctx, items, cfg, films, stats, &ms);
+    if (st == AUR_OK) {
+        e = fo.finish();
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) st = cuda_fail(e, "aur_render(wavefront download)");
+    }
+    cudaFreeAsync(acc, s);
+    cudaStreamSynchronize(s);
+    return st;
+}
+
+}  // namespace aur
+
+extern "C" aur_status aur_render_batch(aur_scene* const* scenes, const aur_render_opts* opts, uint32_t n,
+                                       float* const* films, aur_render_stats* stats) {
+    using namespace aur;
+    if (!scenes || !opts || !films || n == 0) return fail(AUR_ERR_INVALID_ARG, "aur_render_batch: NULL argument");
+    aur_ctx* ctx = scenes[0] ? scenes[0]->ctx : nullptr;
+    if (!ctx) return fail(AUR_ERR_INVALID_ARG, "aur_render_batch: NULL scene");
+    for (uint32_t i = 0; i < n; ++i)
+        if (!scenes[i] || scenes[i]->ctx != ctx || !films[i])
+            return fail(AUR_ERR_INVALID_ARG, "aur_render_batch: scenes must share one context and have films");
+    WfConfig cfg = config_from(&opts[0], WfConfig());
+    aur_status st = check_config(cfg);
+    if (st != AUR_OK) return st;
+    DeviceGuard g(ctx->device);
+    cudaStream_t s = ctx->stream;
+    std::vector<BatchItem> items(n);
+    std::vector<DevOut> outs(n);
+    std::vector<float4*> fl(n);
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+        PathParams p;
+        if ((st = render_options(scenes[i], &opts[i], &p)) != AUR_OK) return st;
+        const uint32_t npix = (uint32_t)scenes[i]->cam.w * scenes[i]->cam.h;
+        total += (uint64_t)npix * p.spp;
+        items[i] = {scenes[i], p, npix, nullptr, nullptr};
+    }
+    if (total >= (1ull << 31)) return fail(AUR_ERR_INVALID_ARG, "aur_render_batch: more than 2^31 paths");
+    cudaError_t e = cudaSuccess;
+    for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) {
+        e = outs[i].init(films[i], sizeof(float4) * items[i].npix, 16, s);
+        fl[i] = (float4*)outs[i].ptr;
+        if (e == cudaSuccess) e = cudaMallocAsync(&items[i].acc_s, sizeof(float4) * 2 * items[i].npix, s);
+        items[i].acc_c = items[i].acc_s + items[i].npix;
+    }
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e == cudaSuccess && wants_tuning(&opts[0])) {
+        // tuned once per (scene count, path count) on this context
+        const uint64_t key = ((uint64_t)n << 40) ^ total;
+        auto it = ctx->wf_batch_tuned.find(key);
+        if (it == ctx->wf_batch_tuned.end()) {
+            WfConfig t;
+            st = autotune(ctx, items, &t);
+            if (st == AUR_OK) it = ctx->wf_batch_tuned.emplace(key, std::array<int, 3>{(int)t.pool, t.block, t.sort}).first;
+        }
+        if (st == AUR_OK) { cfg.pool = (uint32_t)it->second[0]; cfg.block = it->second[1]; cfg.sort = it->second[2]; }
+    }
+    if (e == cudaSuccess && st == AUR_OK) st = wavefront_batch(ctx, items, cfg, fl, stats, &ms);
+    else if (e != cudaSuccess) st = cuda_fail(e, "aur_render_batch");
+    for (uint32_t i = 0; i < n && st == AUR_OK; ++i) {
+        e = outs[i].finish();
+        if (e != cudaSuccess) st = cuda_fail(e, "aur_render_batch(download)");
+    }
+    for (uint32_t i = 0; i < n; ++i) if (items[i].acc_s) cudaFreeAsync(items[i].acc_s, s);
+    cudaStreamSynchronize(s);
+    return st;
+}

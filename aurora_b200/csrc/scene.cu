@@ -79,6 +79,7 @@ static cudaError_t upload(T** dst, const void* src, size_t count, cudaStream_t s
 }
 
 static void scene_free(aur_scene* sc) {
+    --sc->ctx->live;
     cudaStream_t s = sc->ctx->stream;
     cudaStreamSynchronize(s);
     bvh_free_device(&sc->bvh.bvh, s);
@@ -165,7 +166,7 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     sc->ctx = ctx;
     sc->bvh = *tmp;
     sc->bvh.owned_by_scene = true;
-    delete tmp;
+    delete tmp;                      // the scene takes over the BVH's place in ctx->live
     sc->ntri = d->ntri;
     sc->nattr = d->nattr;
     sc->ntexel_floats = texel_floats;
@@ -314,7 +315,7 @@ static aur_status render_plain_impl(aur_scene* sc, const aur_render_opts* o, voi
     cudaError_t e = launch_render_plain(sc->dev(), p, f32, d64, sc->ctx->counters, o->count_work != 0, s);
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) e = f64 ? fo64.finish() : fo.finish();
-    unsigned long long cnt[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long cnt[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, sc->ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     float ms = 0.f;
@@ -331,6 +332,8 @@ static aur_status render_plain_impl(aur_scene* sc, const aur_render_opts* o, voi
         stats->paths = cnt[3];
         stats->node_visits = cnt[4];
         stats->tri_tests = cnt[5];
+        stats->shadow_node_visits = cnt[6];
+        stats->shadow_tri_tests = cnt[7];
         stats->launches = 1;
         stats->kernel_ms = ms;
     }

@@ -194,7 +194,8 @@ def main():
     data = workload(args.small)
     W, H, spp = data.width, data.height, data.render["spp"]
     ctx = ab.Context(local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()            # the library's kernels run on this stream; events are recorded on it
+    torch.cuda.set_stream(stream)
     _abi.check(_abi.lib().aur_ctx_set_stream(ctx.handle, stream.cuda_stream), "aur_ctx_set_stream")
     t0 = time.perf_counter()
     scene = ab.Scene(ctx, data)
@@ -252,24 +253,42 @@ def main():
     else:
         other = {"plain_value": value, "wavefront_value": None, "batched_vs_plain": None}
 
-    # roofline of the dominant kernel: algorithmic bytes from a counting pass (1 spp, untimed)
-    cw = frame(modes[head], count_work=1, spp_=1).stats
-    bytes_per_path = (cw["node_visits"] * 64 + cw["tri_tests"] * 48) / max(cw["paths"], 1)
+    # Roofline of the dominant kernel. Algorithmic bytes come from a counting pass of the
+    # plain renderer (1 spp, untimed): both renderers trace the same rays through the same
+    # BVH, so node visits (64 B) and triangle tests (48 B) per path are the same.
+    cw = frame(_abi.RENDER_PLAIN, count_work=1, spp_=1).stats
+    npaths = max(cw["paths"], 1)
+    closest_bpp = (cw["node_visits"] * 64 + cw["tri_tests"] * 48) / npaths
+    shadow_bpp = (cw["shadow_node_visits"] * 64 + cw["shadow_tri_tests"] * 48) / npaths
     peak, peak_kind = peaks()
-    achieved = bytes_per_path * paths_step / (kms_step / 1000.0) / 1e9
+    if head == "plain":
+        kname, kms, kbytes = "k_render_plain", kms_step, (closest_bpp + shadow_bpp) * paths_step
+        shares = None
+    else:
+        stage = st["stage_ms"]
+        shares = {k: v / max(sum(stage.values()), 1e-9) for k, v in stage.items()}
+        if stage["shadow"] > stage["extend"]:
+            kname, kms, kbytes = "k_shadow", stage["shadow"], shadow_bpp * paths_step
+        else:
+            kname, kms, kbytes = "k_extend", stage["extend"], closest_bpp * paths_step
+    achieved = kbytes / (kms / 1000.0) / 1e9
     traffic = None
     try:
         with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            tj = json.load(f).get(head)
+            tj = json.load(f).get(kname)
             if tj:
                 traffic = tj["dram_bytes_per_path"] * paths_step
     except Exception:
         pass
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "peak_kind": peak_kind, "kernel": "k_render_plain" if head == "plain" else "wavefront",
-            "bytes_per_path": bytes_per_path,
-            "node_visits_per_path": cw["node_visits"] / max(cw["paths"], 1),
-            "tri_tests_per_path": cw["tri_tests"] / max(cw["paths"], 1)}
+            "traffic": traffic, "peak_kind": peak_kind, "kernel": kname, "kernel_ms_per_step": kms,
+            "algorithmic_bytes_per_step": kbytes,
+            "closest_bytes_per_path": closest_bpp, "shadow_bytes_per_path": shadow_bpp,
+            "closest_nodes_per_ray": cw["node_visits"] / max(cw["closest_rays"], 1),
+            "shadow_nodes_per_ray": cw["shadow_node_visits"] / max(cw["shadow_rays"], 1),
+            "stage_shares": shares}
+    if head == "wavefront":
+        roof["wavefront_config"] = st["wf_config"]
 
     # end to end through the public C ABI with host buffers (scene arrays in, image out)
     e2e = None

@@ -64,4 +64,4 @@ def test_record_layouts():
     assert C.sizeof(_abi.Ray) == 32
     assert C.sizeof(_abi.Hit) == 20
     assert C.sizeof(_abi.RenderOpts) == 44
-    assert C.sizeof(_abi.RenderStats) == 64
+    assert C.sizeof(_abi.RenderStats) == 136
