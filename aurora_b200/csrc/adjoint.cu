@@ -1,0 +1,440 @@
+// adjoint.cu — path-replay backpropagation (Vicini, Speierer, Jakob, "Path Replay
+// Backpropagation", SIGGRAPH 2021) for the Aurora path loop. No reference counterpart.
+//
+// Given dLoss/dFilm, every pixel replays its spp camera paths with the same
+// counter-based random numbers as the forward renderer:
+//   pass 1  the forward estimator of Integrator::integrateCameraSample
+//           (integrator.cpp:152-300) with identical arithmetic; it records each
+//           vertex's hit (prim, t, u, v) and the visibility of its next-event
+//           rays in thread-local arrays, and yields the path radiance Lo;
+//   pass 2  re-shades the recorded vertices (no ray tracing) and accumulates
+//             dL/dtheta += delta . [ T_k dD_k/dtheta + L_after,k (dw_k/dtheta) / w_k ]
+//           where D_k is the vertex's next-event estimate, w_k = f cos / pdf its
+//           continuation weight, T_k the throughput and L_after,k = Lo minus the
+//           radiance collected up to and including vertex k.
+// Sampling decisions are detached: pdfs, MIS weights, the Kelemen/metal lobe
+// choice, roulette probabilities and the firefly clamp factor are constants of
+// the derivative (the discrete choices and the clamp make the estimator biased;
+// the continuous parts are unbiased). Memory: O(pixels) — nothing is stored per path.
+//
+// Parameters: per material (diffuse rgb, roughness) and all texels. Diffuse
+// colour drives Lambert lobes (matte, Kelemen's diffuse lobe); roughness drives
+// Cook-Torrance lobes (Kelemen, Cook-Torrance, metal roughnessA); a diffuse
+// texture receives the diffuse gradient of the texel the lookup used. Gradients
+// are summed in FP32 with TwoSum-compensated atomics (shared, then global).
+#include "aur_capi_internal.h"
+
+namespace aur {
+namespace {
+
+constexpr int kAdjBlock = 128;
+constexpr int kAdjMaxDepth = 16;
+constexpr int kAdjMaxMat = 64;
+
+struct VtxRec { int prim; float t, u, v; uint32_t vis; };
+
+// atomic add with the exact rounding error of that addition sent to a compensation slot
+__device__ __forceinline__ void comp_add(float* sum, float* comp, float x) {
+    if (x == 0.f) return;
+    const float old = atomicAdd(sum, x);
+    const float t = old + x;                        // what the atomic stored
+    const float bp = t - old;
+    const float err = (old - (t - bp)) + (x - bp);  // TwoSum(old, x) error
+    if (err != 0.f) atomicAdd(comp, err);
+}
+
+// ln D derivative w.r.t. roughness r of the Beckmann term, with tan^2(alpha) given
+// and the reference's max(0.001, r^2) floor (eval uses r^2 unfloored).
+__device__ __forceinline__ float dlnD_dr(float r, float tan2, bool floored) {
+    const float r2 = r * r;
+    if (floored && r2 <= 0.001f) return 0.f;
+    return 2.f * tan2 / (r2 * r) - 2.f / r;
+}
+__device__ __forceinline__ float tan2_of(float ndoth) {
+    const float t = xtanf(xacosf(ndoth));
+    return t * t;
+}
+
+// d ln f / d roughness of a Cook-Torrance sample (cookTorrance.cpp:47-99): the sampled
+// half vector is normalize(L + V); a clamped D (>= 1000) or the 0.001 floor on r^2
+// makes the sample's colour independent of roughness.
+__device__ __forceinline__ float sample_dlnD(const Brdf& b, const Frame& f, const BrdfSample& bs) {
+    const float3 H = normalize(bs.dir + f.V);
+    const float ndoth = dot(f.N, H);
+    const float tana = ndoth > 0.999f ? 0.f : xtanf(xacosf(ndoth));
+    if (ct_d(b.rough, ndoth, tana) >= 1000.f) return 0.f;
+    return dlnD_dr(b.rough, tana * tana, true);
+}
+
+// Next-event estimation of one vertex (integrateDirect with integrateDirectLight /
+// integrateDirectMIS). kTrace: traces the shadow rays and records their visibility
+// in *vis; otherwise replays `vis`. With kGrad it also returns dD/dtheta of the lobe's
+// parameter: per channel d/d(diffuse_c) for a Lambert lobe, d/d(roughness_eff) for a
+// Cook-Torrance lobe (replicated in all channels).
+template <bool kTrace, bool kGrad>
+__device__ __forceinline__ float3 direct(const DevScene& sc, const Frame& f, const Brdf& brdf, const PathRng& rng,
+                                         int vtx, RayCounts& rc, uint32_t* vis, float3* dD) {
+    float3 res = mk(0.f, 0.f, 0.f), dres = res;
+    if (kGrad) *dD = res;
+    if (brdf.lobe != LOBE_MATTE && brdf.lobe != LOBE_SPEC) return res;
+    int nvis;
+    const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
+    if (li < 0) return res;
+    const Light L = sc.sh.lights[li];
+    const LightSample ls = light_sample(L, f.P, rng.u(vertex_dim(vtx, kDimLightSample)),
+                                        rng.u(vertex_dim(vtx, kDimLightSample + 1)));
+    float cost = dot(f.N, ls.dir);
+    if (brdf.lobe == LOBE_MATTE) {
+        if (cost >= 0.f && ls.pdf > 0.f) {
+            bool open;
+            if (kTrace) { ++rc.shadow; open = !bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work); if (open) *vis |= 1u; }
+            else open = (*vis & 1u) != 0;
+            if (open) {
+                res += cdiv((ls.color * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
+                if (kGrad && dot(ls.dir, f.N) > 0.f) dres += cdiv((ls.color * kInvPiMacro) * cost, ls.pdf);
+            }
+        }
+    } else {
+        if (cost > 0.f && ls.pdf > 0.f) {
+            const float bp = brdf_pdf(brdf, ls.dir, f.V, f.N);
+            if (bp > 0.f) {
+                bool open;
+                if (kTrace) { ++rc.shadow; open = !bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work); if (open) *vis |= 1u; }
+                else open = (*vis & 1u) != 0;
+                if (open) {
+                    const float w = power_heuristic(ls.pdf, bp);
+                    const float3 c0 = cdiv(((ls.color * w) * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
+                    res += c0;
+                    if (kGrad) {
+                        const float3 H = normalize(ls.dir + f.V);
+                        dres += c0 * dlnD_dr(brdf.rough, tan2_of(dot(H, f.N)), false);
+                    }
+                }
+            }
+        }
+        const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimMisBrdf)),
+                                          rng.u(vertex_dim(vtx, kDimMisBrdf + 1)));
+        cost = dot(f.N, bs.dir);
+        if (cost > 0.f) {
+            float maxt = bs.maxt;
+            const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
+            if (lp > 0.f && bs.pdf > 0.f) {
+                bool open;
+                if (kTrace) { ++rc.shadow; open = !bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.shadow_work); if (open) *vis |= 2u; }
+                else open = (*vis & 2u) != 0;
+                if (open) {
+                    const float w = power_heuristic(bs.pdf, lp);
+                    const float3 c1 = cdiv(((bs.color * w) * L.le) * cost, bs.pdf);
+                    res += c1;
+                    if (kGrad) dres += c1 * sample_dlnD(brdf, f, bs);
+                }
+            }
+        }
+    }
+    if (kGrad) *dD = dres * (float)nvis;
+    return res * (float)nvis;
+}
+
+// d A / d roughness of the Kelemen directional-albedo lookup (kelemen_albedo): the
+// lookup is linear in roughness * 31 between the two columns it reads.
+__device__ __forceinline__ float kelemen_dalbedo_dr(const float* table, float costheta, float roughness) {
+    int i = aur_floor(costheta * (kAlbedoCos - 1));
+    int ra = aur_floor(roughness * (kAlbedoRough - 1));
+    int rb = ra + 1 > kAlbedoRough - 1 ? ra + 1 : kAlbedoRough - 1;
+    i = i < 0 ? 0 : (i > kAlbedoCos - 1 ? kAlbedoCos - 1 : i);
+    ra = ra < 0 ? 0 : (ra > kAlbedoRough - 1 ? kAlbedoRough - 1 : ra);
+    rb = rb > kAlbedoRough - 1 ? kAlbedoRough - 1 : rb;
+    const int i1 = i + 1 < kAlbedoCos - 1 ? i + 1 : kAlbedoCos - 1;
+    const float mixc = costheta * (kAlbedoCos - 1) - (float)i;
+    const float resA = (1.f - mixc) * table[i * kAlbedoRough + ra] + mixc * table[i1 * kAlbedoRough + ra];
+    const float resB = (1.f - mixc) * table[i * kAlbedoRough + rb] + mixc * table[i1 * kAlbedoRough + rb];
+    return (resB - resA) * (float)(kAlbedoRough - 1);
+}
+
+// Score-function factor d ln P(chosen lobe) / d roughness of Kelemen's lobe choice
+// (kelemenMaterial.cpp:236-253): P(spec) = min(1, A(cos, r_eff)), P(diffuse) = 1 - A.
+__device__ __forceinline__ float kelemen_score(const ShadeScene& sh, const Material& m, const Frame& f, const Brdf& b,
+                                               bool matte) {
+    float r = m.rough;
+    if (matte) r = caustic_blur(r);
+    float c = dot(f.N, f.V);
+    c = c < 0.f ? 0.f : (c > 1.f ? 1.f : c);
+    const float* table = sh.albedo + (size_t)m.table * (kAlbedoCos * kAlbedoRough);
+    const float A = kelemen_albedo(table, c, r);
+    const float dA = kelemen_dalbedo_dr(table, c, r) * (matte ? (float)(1.0 - 0.2) : 1.f);
+    if (b.lobe == LOBE_SPEC) return A < 1.f && A > 0.f ? dA / A : 0.f;
+    return A < 1.f ? -dA / (1.f - A) : 0.f;
+}
+
+// Which parameter a vertex's lobe depends on.
+struct ParamRef {
+    int kind;        // 0 none, 1 diffuse colour of material `index`, 2 texel block `index` (3 floats), 3 roughness
+    int index;
+    float dr;        // roughness: d r_eff / d r (caustic blur on matte paths)
+};
+
+__device__ __forceinline__ ParamRef param_of(const ShadeScene& sh, int mat_id, const Brdf& b, const Frame& f,
+                                             bool matte, float lobe_u) {
+    ParamRef p{0, 0, 0.f};
+    const Material m = sh.mats[mat_id];
+    if (b.lobe == LOBE_MATTE) {
+        if (m.type != MAT_MATTE && m.type != MAT_KELEMEN) return p;
+        if (m.diff_tex >= 0) {
+            const Texture t = sh.texs[m.diff_tex];
+            const float fs = f.su - (float)aur_floor(f.su);
+            const float ft = 1.f - (f.sv - (float)aur_floor(f.sv));
+            int x = aur_floor(fs * (float)t.w), y = aur_floor(ft * (float)t.h);
+            if (y == t.h) y -= 1;
+            if (x == t.w) x -= 1;
+            x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
+            y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
+            p.kind = 2;
+            p.index = (t.offset / 3) + y * t.w + x;
+        } else {
+            p.kind = 1;
+            p.index = mat_id;
+        }
+        return p;
+    }
+    if (b.lobe == LOBE_SPEC && m.rough_tex < 0 &&
+        (m.type == MAT_KELEMEN || m.type == MAT_COOKTORRANCE || (m.type == MAT_METAL && lobe_u > m.mix))) {
+        p.kind = 3;
+        p.index = mat_id;
+        p.dr = matte ? (float)(1.0 - 0.2) : 1.f;
+    }
+    return p;
+}
+
+__global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p, const float4* __restrict__ dfilm,
+                                                       int nmat, float* g_mat, float* g_mat_c, float* g_tex,
+                                                       float* g_tex_c, unsigned long long* counters) {
+    __shared__ float s_g[kAdjMaxMat * 4], s_c[kAdjMaxMat * 4];
+    for (int i = threadIdx.x; i < nmat * 4; i += blockDim.x) { s_g[i] = 0.f; s_c[i] = 0.f; }
+    __syncthreads();
+    const int npix = sc.cam.w * sc.cam.h;
+    const int pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    RayCounts rc;
+    if (pixel < npix) {
+        const float4 df = dfilm[pixel];
+        const float inv = 1.f / (float)p.spp;
+        const float3 delta = mk(df.x * inv, df.y * inv, df.z * inv);
+        const int px = pixel % sc.cam.w, py = pixel / sc.cam.w;
+        PathRng rng;
+        rng.key = seed_key(p.seed);
+        const bool any = delta.x != 0.f || delta.y != 0.f || delta.z != 0.f;
+        for (int s = 0; any && s < p.spp; ++s) {
+            rng.base = path_base((uint32_t)pixel, (uint32_t)(p.sample_offset + s));
+            // ---------------- pass 1: forward replay, recording hits and visibility
+            VtxRec rec[kAdjMaxDepth];
+            int nv = 0;
+            float3 Lo = mk(0.f, 0.f, 0.f);
+            {
+                RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+                Hit h;
+                ++rc.closest;
+                if (bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+                    float3 T = mk(1.f, 1.f, 1.f);
+                    float cont = 1.f;
+                    bool matte = false;
+                    int kind = RAY_CAMERA, bounces = 0;
+                    for (int vtx = 0; vtx < p.max_depth; ++vtx) {
+                        rec[vtx] = {h.prim, h.t, h.u, h.v, 0u};
+                        nv = vtx + 1;
+                        const Frame f = hit_frame(sc.sh, h.prim, h.t, h.u, h.v, ray.o, ray.d, true);
+                        const Attr at = sc.sh.attrs[f.attr];
+                        if (kind == RAY_DIFFUSE) matte = true;
+                        if (kind == RAY_CAMERA) Lo += T * at.emission;
+                        const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
+                                                   rng.u(vertex_dim(vtx, kDimLobe)));
+                        Lo += direct<true, false>(sc, f, brdf, rng, vtx, rc, &rec[vtx].vis, nullptr) * T;
+                        const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
+                                                          rng.u(vertex_dim(vtx, kDimBrdf + 1)));
+                        if (bs.pdf <= 0.f) break;
+                        const float cosl = dot(f.N, bs.dir);
+                        T *= cdiv(bs.color * cosl, bs.pdf);
+                        if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
+                        if (is_black(T)) break;
+                        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
+                        if (bounces > p.min_depth) {
+                            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
+                            T = cdiv(T, cont);
+                        }
+                        ++bounces;
+                        if (vtx + 1 >= p.max_depth) break;
+                        ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
+                        ++rc.closest;
+                        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) break;
+                    }
+                }
+            }
+            if (nv == 0 || !isfinite(Lo.x) || !isfinite(Lo.y) || !isfinite(Lo.z)) continue;
+            float clampf = 1.f;             // firefly clamp factor (detached)
+            {
+                float3 c = Lo;
+                for (int k = 0; k < 64 && (c.x > kFirefly || c.y > kFirefly || c.z > kFirefly); ++k) { c *= 0.2f; clampf *= 0.2f; }
+            }
+            const float3 dp = delta * clampf;
+            // ---------------- pass 2: re-shade the recorded vertices, accumulate gradients
+            RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+            float3 T = mk(1.f, 1.f, 1.f), collected = mk(0.f, 0.f, 0.f);
+            float cont = 1.f;
+            bool matte = false;
+            int kind = RAY_CAMERA, bounces = 0;
+            for (int vtx = 0; vtx < nv; ++vtx) {
+                const VtxRec r = rec[vtx];
+                const Frame f = hit_frame(sc.sh, r.prim, r.t, r.u, r.v, ray.o, ray.d, true);
+                const Attr at = sc.sh.attrs[f.attr];
+                if (kind == RAY_DIFFUSE) matte = true;
+                if (kind == RAY_CAMERA) collected += T * at.emission;
+                const float lobe_u = rng.u(vertex_dim(vtx, kDimLobe));
+                const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte, lobe_u);
+                const ParamRef pr = param_of(sc.sh, at.material, brdf, f, matte, lobe_u);
+                uint32_t vis = r.vis;
+                float3 dD;
+                const float3 D = direct<false, true>(sc, f, brdf, rng, vtx, rc, &vis, &dD);
+                collected += D * T;
+                const float3 gdir = T * dD;
+                const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
+                                                  rng.u(vertex_dim(vtx, kDimBrdf + 1)));
+                float3 gcont = mk(0.f, 0.f, 0.f);
+                float3 w = mk(0.f, 0.f, 0.f);
+                const bool cont_ok = bs.pdf > 0.f;
+                const float3 after = Lo - collected;
+                const Material mat = sc.sh.mats[at.material];
+                if (mat.type == MAT_KELEMEN && mat.refl < 1.f && mat.rough_tex < 0) {
+                    // the lobe choice depends on roughness: score-function term on the subtree radiance
+                    const float score = kelemen_score(sc.sh, mat, f, brdf, matte);
+                    const float3 sub = dp * (D * T + after);
+                    comp_add(&s_g[4 * at.material + 3], &s_c[4 * at.material + 3], score * (sub.x + sub.y + sub.z));
+                }
+                if (cont_ok && pr.kind != 0) {
+                    const float cosl = dot(f.N, bs.dir);
+                    w = cdiv(bs.color * cosl, bs.pdf);
+                    if (pr.kind == 3) {
+                        const float g = sample_dlnD(brdf, f, bs);   // dw/w = d ln f
+                        gcont = after * g;
+                    } else {
+                        const float dw = kInvPiMacro * cosl / bs.pdf;  // d w_c / d diffuse_c
+                        gcont = mk(w.x != 0.f ? after.x * dw / w.x : 0.f, w.y != 0.f ? after.y * dw / w.y : 0.f,
+                                   w.z != 0.f ? after.z * dw / w.z : 0.f);
+                    }
+                }
+                if (pr.kind == 1 || pr.kind == 2) {
+                    const float3 g = dp * (gdir + gcont);
+                    if (pr.kind == 1) {
+                        comp_add(&s_g[4 * pr.index + 0], &s_c[4 * pr.index + 0], g.x);
+                        comp_add(&s_g[4 * pr.index + 1], &s_c[4 * pr.index + 1], g.y);
+                        comp_add(&s_g[4 * pr.index + 2], &s_c[4 * pr.index + 2], g.z);
+                    } else {
+                        comp_add(&g_tex[3 * pr.index + 0], &g_tex_c[3 * pr.index + 0], g.x);
+                        comp_add(&g_tex[3 * pr.index + 1], &g_tex_c[3 * pr.index + 1], g.y);
+                        comp_add(&g_tex[3 * pr.index + 2], &g_tex_c[3 * pr.index + 2], g.z);
+                    }
+                } else if (pr.kind == 3) {
+                    const float3 g = dp * (gdir * pr.dr + gcont * pr.dr);
+                    comp_add(&s_g[4 * pr.index + 3], &s_c[4 * pr.index + 3], g.x + g.y + g.z);
+                }
+                // the forward update, identical to pass 1
+                if (!cont_ok) break;
+                const float cosl = dot(f.N, bs.dir);
+                T *= cdiv(bs.color * cosl, bs.pdf);
+                if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
+                if (is_black(T)) break;
+                kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
+                if (bounces > p.min_depth) {
+                    if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
+                    T = cdiv(T, cont);
+                }
+                ++bounces;
+                ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
+            }
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < nmat * 4; i += blockDim.x) {
+        comp_add(&g_mat[i], &g_mat_c[i], s_g[i]);
+        comp_add(&g_mat[i], &g_mat_c[i], s_c[i]);
+    }
+    unsigned long long v[3] = {rc.closest, rc.shadow, pixel < npix ? (unsigned long long)p.spp : 0ull};
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
+    if ((threadIdx.x & 31) == 0)
+        for (int k = 0; k < 3; ++k) atomicAdd(&counters[k], v[k]);
+}
+
+__global__ void k_add_comp(float* g, const float* c, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) g[i] += c[i];
+}
+
+}  // namespace
+}  // namespace aur
+
+using namespace aur;
+
+extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o, const float* dfilm, float* grad_mat,
+                                         float* grad_tex, aur_render_stats* stats) {
+    if (!sc || !o || !dfilm || !grad_mat) return fail(AUR_ERR_INVALID_ARG, "aur_render_adjoint: NULL argument");
+    if (sc->ntexel_floats && !grad_tex) return fail(AUR_ERR_INVALID_ARG, "aur_render_adjoint: grad_tex is NULL");
+    PathParams p;
+    aur_status st = render_options(sc, o, &p);
+    if (st != AUR_OK) return st;
+    if (o->max_depth > kAdjMaxDepth) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: max_depth above 16");
+    const int nmat = (int)sc->h_mats.size();
+    if (nmat > kAdjMaxMat) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: more than 64 materials");
+    DeviceGuard g(sc->ctx->device);
+    cudaStream_t s = sc->ctx->stream;
+    const size_t npix = (size_t)sc->cam.w * sc->cam.h;
+    const int ntex = (int)sc->ntexel_floats;
+    DevIn din;
+    DevOut gm, gt;
+    float *cm = nullptr, *ct = nullptr;
+    cudaError_t e = din.init(dfilm, sizeof(float4) * npix, 16, s);
+    if (e == cudaSuccess) e = gm.init(grad_mat, sizeof(float) * 4 * nmat, 4, s);
+    if (e == cudaSuccess && ntex) e = gt.init(grad_tex, sizeof(float) * ntex, 4, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&cm, sizeof(float) * (4 * nmat + ntex), s);
+    ct = cm ? cm + 4 * nmat : nullptr;
+    if (e == cudaSuccess) e = cudaMemsetAsync(gm.ptr, 0, sizeof(float) * 4 * nmat, s);
+    if (e == cudaSuccess && ntex) e = cudaMemsetAsync(gt.ptr, 0, sizeof(float) * ntex, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(cm, 0, sizeof(float) * (4 * nmat + ntex), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(sc->ctx->counters, 0, sizeof(unsigned long long) * 8, s);
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaEventRecord(e0, s);
+    if (e == cudaSuccess) {
+        k_adjoint<<<(unsigned)((npix + kAdjBlock - 1) / kAdjBlock), kAdjBlock, 0, s>>>(
+            sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm, ntex ? (float*)gt.ptr : nullptr, ct,
+            sc->ctx->counters);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) {
+        k_add_comp<<<(4 * nmat + 255) / 256, 256, 0, s>>>((float*)gm.ptr, cm, 4 * nmat);
+        if (ntex) k_add_comp<<<(ntex + 255) / 256, 256, 0, s>>>((float*)gt.ptr, ct, ntex);
+        e = cudaGetLastError();
+    }
+    cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = gm.finish();
+    if (e == cudaSuccess && ntex) e = gt.finish();
+    unsigned long long cnt[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, sc->ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    float ms = 0.f;
+    if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (cm) cudaFreeAsync(cm, s);
+    if (e != cudaSuccess) return cuda_fail(e, "aur_render_adjoint");
+    if (stats) {
+        *stats = aur_render_stats{};
+        stats->closest_rays = cnt[0];
+        stats->shadow_rays = cnt[1];
+        stats->paths = cnt[2];
+        stats->camera_rays = cnt[2];
+        stats->launches = ntex ? 3 : 2;
+        stats->kernel_ms = ms;
+    }
+    return AUR_OK;
+}

@@ -17,6 +17,7 @@ struct aur_ctx {
     cudaStream_t work_stream = nullptr;        // non-blocking stream for captured work (wavefront graphs)
     cudaEvent_t ev_order = nullptr;            // orders work_stream after `stream`
     std::map<uint64_t, std::array<int, 3>> wf_batch_tuned;   // autotuned batch configs (pool, block, sort)
+    std::map<uint64_t, std::array<int, 3>> wf_scene_tuned;   // autotuned configs by scene signature
     int live = 0;                              // BVHs and scenes created on this context and not destroyed
 };
 

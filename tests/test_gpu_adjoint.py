@@ -1,0 +1,112 @@
+"""Path-replay adjoint against central finite differences with common random numbers,
+and the torch.autograd binding."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def setup(ctx, res=48):
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    data = scenes.texture_scene(res, res)
+    scene = ab.Scene(ctx, data)
+    rng = np.random.default_rng(17)
+    w = rng.normal(size=(res, res, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    return data, scene, w
+
+
+def loss(scene, params, texels, w, spp, seed=2):
+    import aurora_b200 as ab
+    from aurora_b200 import _abi
+    scene.set_params(params, texels)
+    film = scene.render(ab.render_opts(spp, 6, 6, seed, mode=_abi.RENDER_WAVEFRONT)).film
+    return float(np.sum(film.astype(np.float64) * w))
+
+
+def adjoint(scene, w, spp, seed=2):
+    import aurora_b200 as ab
+    gm, gt, stats = scene.adjoint(ab.render_opts(spp, 6, 6, seed), w)
+    return gm.astype(np.float64), gt.astype(np.float64), stats
+
+
+def test_albedo_and_texel_gradients_match_fd(ctx):
+    """Lambert sampling does not depend on the diffuse colour, so with common random numbers the
+    estimator is smooth in it and the adjoint equals the finite difference sample by sample."""
+    data, scene, w = setup(ctx)
+    p0, t0 = data.material_params(), data.texels()
+    spp = 16
+    gm, gt, stats = adjoint(scene, w, spp)
+    assert stats["paths"] == 48 * 48 * spp
+    h = 1e-3
+    rng = np.random.default_rng(5)
+    checks = []
+    for c in range(3):                      # Kelemen sphere diffuse colour (material 1)
+        v = np.zeros_like(p0); v[1, c] = 1.0
+        checks.append((v, None))
+    for _ in range(2):                      # random texel directions
+        vt = rng.normal(size=t0.shape).astype(np.float32)
+        checks.append((None, vt))
+    for v, vt in checks:
+        pp = p0 + h * v if v is not None else p0
+        pm = p0 - h * v if v is not None else p0
+        tp = t0 + h * vt if vt is not None else t0
+        tm = t0 - h * vt if vt is not None else t0
+        fd = (loss(scene, pp, tp, w, spp) - loss(scene, pm, tm, w, spp)) / (2 * h)
+        ad = (np.sum(gm * v) if v is not None else 0.0) + (np.sum(gt * vt) if vt is not None else 0.0)
+        assert abs(ad - fd) <= 0.02 * abs(fd) + 1e-3, (ad, fd)
+    scene.set_params(p0, t0)
+
+
+def test_roughness_gradient_matches_fd(ctx):
+    """Roughness changes the sampled directions and the Kelemen lobe choice, so the adjoint
+    and the finite difference agree in expectation only: both are estimated over 8
+    independent sample batches and compared within 3 standard errors. h = 1e-3 keeps
+    r +- h inside one cell of the albedo table (the reference's lookup jumps at r = k/31)."""
+    import aurora_b200 as ab
+    from aurora_b200 import _abi
+    data, scene, w = setup(ctx, res=32)
+    p0, t0 = data.material_params(), data.texels()
+    h, spp, batches = 1e-3, 512, 8
+    v = np.zeros_like(p0); v[1, 3] = 1.0
+    ads, fds = [], []
+    for b in range(batches):
+        o = dict(sample_offset=b * spp)
+        gm, _, _ = scene.adjoint(ab.render_opts(spp, 6, 6, 2, **o), w)
+        ads.append(float(gm[1, 3]))
+        vals = []
+        for sgn in (1, -1):
+            scene.set_params(p0 + sgn * h * v, t0)
+            film = scene.render(ab.render_opts(spp, 6, 6, 2, mode=_abi.RENDER_WAVEFRONT, **o)).film
+            vals.append(float(np.sum(film.astype(np.float64) * w)))
+        scene.set_params(p0, t0)
+        fds.append((vals[0] - vals[1]) / (2 * h))
+    ad, fd = np.mean(ads), np.mean(fds)
+    se = np.sqrt(np.var(ads, ddof=1) / batches + np.var(fds, ddof=1) / batches)
+    print(f"\nroughness: adjoint {ad:.5g} +- {np.std(ads, ddof=1) / np.sqrt(batches):.3g}, "
+          f"fd {fd:.5g} +- {np.std(fds, ddof=1) / np.sqrt(batches):.3g}")
+    assert abs(ad - fd) <= 3 * se + 0.02 * abs(fd), (ad, fd, se)
+
+
+def test_autograd_function(ctx):
+    import torch
+    from aurora_b200.pyaurora import AuroraRender
+    data, scene, w = setup(ctx, res=32)
+    params = torch.tensor(data.material_params(), device="cuda", requires_grad=True)
+    texels = torch.tensor(data.texels(), device="cuda", requires_grad=True)
+    opts = dict(spp=8, max_depth=6, seed=2)
+    img = AuroraRender.apply(params, texels, scene, opts)
+    wt = torch.tensor(w, device="cuda")
+    (img * wt).sum().backward()
+    gm, gt, _ = adjoint(scene, w, 8)
+    np.testing.assert_allclose(params.grad.cpu().numpy(), gm, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(texels.grad.cpu().numpy(), gt, rtol=1e-5, atol=1e-6)
+    assert img.shape == (32, 32, 4)
+
+
+def test_adjoint_is_deterministic(ctx):
+    data, scene, w = setup(ctx, res=32)
+    a = adjoint(scene, w, 8)
+    b = adjoint(scene, w, 8)
+    assert np.allclose(a[0], b[0], rtol=1e-5, atol=1e-7) and np.allclose(a[1], b[1], rtol=1e-5, atol=1e-7)
