@@ -38,6 +38,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--mode", default="auto", choices=["auto", "plain", "wavefront"])
+    p.add_argument("--profile", action="store_true",
+                   help="render two 1-spp frames of the workload with a fixed wavefront configuration "
+                        "(pool 2^20, block 128, sort on) and exit: the small case for ncu captures")
     return p.parse_args()
 
 
@@ -174,10 +177,30 @@ def run_reference(args):
     return 0
 
 
+def run_profile_case(args):
+    """Two 1-spp frames of the full-size scene (about 1 GB on the device), no timing output."""
+    import aurora_b200 as ab
+    from aurora_b200 import _abi
+    data = workload(args.small)
+    ctx = ab.Context(0)
+    scene = ab.Scene(ctx, data)
+    r = data.render
+    mode = _abi.RENDER_PLAIN if args.mode == "plain" else _abi.RENDER_WAVEFRONT
+    for k in range(2):
+        res = scene.render(ab.render_opts(1, r["max_depth"], r["min_depth"], r["seed"], mode=mode, sample_offset=k,
+                                          wf_pool=1 << 20, wf_block=128, wf_sort=1))
+    print(json.dumps({"profile_case": data.name, "tris": data.ntri, "mode": args.mode, "stats": res.stats}))
+    scene.close()
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile_case(args)
     import torch
     import aurora_b200 as ab
     from aurora_b200 import _abi
