@@ -30,7 +30,11 @@
 namespace aur {
 namespace {
 
-enum : uint32_t { PS_EMPTY = 0, PS_ACTIVE = 1, PS_DONE = 2 };
+enum : uint32_t { PS_EMPTY = 0, PS_ACTIVE = 1, PS_DONE = 2, PS_MASK = 3, PS_PENDING = 4 };
+// lane refill: a warp takes new rays once this many lanes are idle, and every lane
+// advances its traversal by up to kSteps nodes/leaves between refill checks
+constexpr int kRefill = 16;
+constexpr int kSteps = 16;
 enum : int { B_MISS = 0, B_MATTE = 1, B_KELEMEN = 2, B_CT = 3, B_METAL = 4, B_CONST = 5, kBuckets = 6 };
 // counters
 enum : int {
@@ -49,7 +53,8 @@ struct WfScene {
 struct WfPool {
     float4 *ray_o, *ray_d, *tp, *lo, *hit, *sh_p, *sh_d0, *sh_d1, *sh_c0, *sh_c1, *sh_t;
     uint4* id;
-    uint32_t* state;
+    uint32_t* state;            // PS_* in the low bits, PS_PENDING when next-event rays are in flight
+    uint32_t* sh_vis;           // bit k: next-event ray k of the slot is unoccluded
     uint32_t *q_ext0, *q_ext1, *q_sort, *q_shadow;
     uint32_t* ctr;
     unsigned long long* rays;   // [0] closest-hit rays, [1] shadow rays
@@ -107,6 +112,21 @@ __global__ void k_regen(WfPool w, int in_q) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < w.P;
         uint32_t st = valid ? w.state[i] : (uint32_t)PS_ACTIVE;
+        if (st & PS_PENDING) {
+            // next-event estimate of the last vertex: Lo += ((vis0 c0 + vis1 c1) nvis) T, the
+            // plain kernel's order of operations (integrate_direct)
+            const uint32_t vis = w.sh_vis[i];
+            const float4 c0 = w.sh_c0[i], c1 = w.sh_c1[i], t = w.sh_t[i];
+            const float nvis = w.sh_p[i].w;
+            float3 res = mk(0.f, 0.f, 0.f);
+            if (vis & 1u) res += mk(c0.x, c0.y, c0.z);
+            if (vis & 2u) res += mk(c1.x, c1.y, c1.z);
+            float4 lo = w.lo[i];
+            const float3 add = (res * nvis) * mk(t.x, t.y, t.z);
+            lo.x += add.x; lo.y += add.y; lo.z += add.z;
+            w.lo[i] = lo;
+            st &= ~PS_PENDING;
+        }
         if (st == PS_DONE) {
             const uint4 id = w.id[i];
             const WfScene& S = w.scenes[id.x];
@@ -149,6 +169,16 @@ __global__ void k_regen(WfPool w, int in_q) {
 }
 
 // ------------------------------------------------------------------ extend
+__device__ __forceinline__ int bucket_of(const ShadeScene& sh, int prim) {
+    if (prim < 0) return B_MISS;
+    const int mt = sh.mats[sh.attrs[sh.tri_attr[prim]].material].type;
+    return mt == MAT_MATTE ? B_MATTE : mt == MAT_KELEMEN ? B_KELEMEN : mt == MAT_COOKTORRANCE ? B_CT
+         : mt == MAT_METAL ? B_METAL : B_CONST;
+}
+
+// Closest hit for the extension queue. Each lane keeps a resumable traversal;
+// finished lanes are refilled from the queue (one atomic per warp) while the
+// others continue, so a warp is not held up by its slowest ray.
 template <bool kSort>
 __global__ void k_extend(WfPool w, int in_q) {
     const uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
@@ -164,33 +194,53 @@ __global__ void k_extend(WfPool w, int in_q) {
         w.ctr[C_CUR_SORT] = 0;
         w.rays[0] += n;
     }
+    int stack[kTraversalStack];
+    TraceState<false> ts;
+    const BvhNode* nodes = nullptr;
+    const BvhTri* tris = nullptr;
+    const WfScene* S = nullptr;
+    uint32_t slot = 0;
+    bool has = false, exhausted = false;
     while (true) {
-        const uint32_t b = warp_fetch(&w.ctr[C_CUR_EXT]);
-        if (b >= n) break;
-        const uint32_t k = b + lane_id();
-        int bucket = -1;
-        if (k < n) {
-            const uint32_t slot = qin[k];
-            const float4 o = w.ray_o[slot], d = w.ray_d[slot];
-            const WfScene& S = w.scenes[w.id[slot].x];
-            Hit h;
-            TraceWork work;
-            const bool hit = bvh_closest(S.sc.nodes, S.sc.tris, mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, d.w, &h, work);
-            w.hit[slot] = make_float4(h.t, h.u, h.v, __int_as_float(hit ? h.prim : -1));
-            if (kSort) {
-                bucket = B_MISS;
-                if (hit) {
-                    const int mt = S.sc.sh.mats[S.sc.sh.attrs[S.sc.sh.tri_attr[h.prim]].material].type;
-                    bucket = mt == MAT_MATTE ? B_MATTE : mt == MAT_KELEMEN ? B_KELEMEN : mt == MAT_COOKTORRANCE ? B_CT
-                           : mt == MAT_METAL ? B_METAL : B_CONST;
+        const bool need = !has && !exhausted;
+        const uint32_t m = __ballot_sync(0xffffffffu, need);
+        const uint32_t act = __ballot_sync(0xffffffffu, has);
+        if (m && (__popc(m) >= kRefill || act == 0)) {
+            const int leader = __ffs(m) - 1;
+            uint32_t b = 0;
+            if ((int)lane_id() == leader) b = atomicAdd(&w.ctr[C_CUR_EXT], (uint32_t)__popc(m));
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (need) {
+                const uint32_t k = b + __popc(m & lanemask_lt());
+                if (k < n) {
+                    slot = qin[k];
+                    S = &w.scenes[w.id[slot].x];
+                    nodes = S->sc.nodes;
+                    tris = S->sc.tris;
+                    const float4 o = w.ray_o[slot], d = w.ray_d[slot];
+                    ts.begin(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, d.w);
+                    has = true;
+                } else {
+                    exhausted = true;
                 }
             }
         }
-        if (kSort) {
-            // per-bucket counts, one atomic per (warp, bucket)
-            const uint32_t active = __ballot_sync(0xffffffffu, bucket >= 0);
+        if (__ballot_sync(0xffffffffu, has || !exhausted) == 0) break;
+        bool done = false;
+        if (has) {
+            for (int k = 0; k < kSteps; ++k)
+                if (ts.step(nodes, tris, stack)) { done = true; break; }
+        }
+        int bucket = -1;
+        if (done) {
+            w.hit[slot] = make_float4(ts.tbest, ts.bu, ts.bv, __int_as_float(ts.best));
+            if (kSort) bucket = bucket_of(S->sc.sh, ts.best);
+            has = false;
+        }
+        if (kSort) {   // per-bucket counts, one atomic per (warp, bucket)
+            const uint32_t fin = __ballot_sync(0xffffffffu, bucket >= 0);
             if (bucket >= 0) {
-                const uint32_t peers = __match_any_sync(active, bucket);
+                const uint32_t peers = __match_any_sync(fin, bucket);
                 if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&w.ctr[C_BUCKET + bucket], (uint32_t)__popc(peers));
             }
         }
@@ -215,15 +265,8 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
         uint32_t slot = 0;
         if (k < n) {
             slot = qin[k];
-            const float4 h = w.hit[slot];
-            const int prim = __float_as_int(h.w);
-            bucket = B_MISS;
-            if (prim >= 0) {
-                const WfScene& S = w.scenes[w.id[slot].x];
-                const int mt = S.sc.sh.mats[S.sc.sh.attrs[S.sc.sh.tri_attr[prim]].material].type;
-                bucket = mt == MAT_MATTE ? B_MATTE : mt == MAT_KELEMEN ? B_KELEMEN : mt == MAT_COOKTORRANCE ? B_CT
-                       : mt == MAT_METAL ? B_METAL : B_CONST;
-            }
+            const int prim = __float_as_int(w.hit[slot].w);
+            bucket = bucket_of(w.scenes[w.id[slot].x].sc.sh, prim);
         }
         const uint32_t active = __ballot_sync(0xffffffffu, bucket >= 0);
         if (bucket >= 0) {
@@ -251,7 +294,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
         const uint32_t b = warp_fetch(&w.ctr[C_CUR_SHADE]);
         if (b >= n) break;
         const uint32_t k = b + lane_id();
-        bool push_ext = false, push_sh = false;
+        bool push_ext = false, push_sh0 = false, push_sh1 = false;
         uint32_t slot = 0;
         if (k < n) {
             slot = qin[k];
@@ -330,10 +373,12 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                             w.sh_p[slot] = make_float4(f.P.x, f.P.y, f.P.z, (float)nvis);
                             w.sh_d0[slot] = make_float4(d0.x, d0.y, d0.z, m0);
                             w.sh_d1[slot] = make_float4(d1.x, d1.y, d1.z, m1);
-                            w.sh_c0[slot] = make_float4(c0.x, c0.y, c0.z, r0 ? 1.f : 0.f);
-                            w.sh_c1[slot] = make_float4(c1.x, c1.y, c1.z, r1 ? 1.f : 0.f);
+                            w.sh_c0[slot] = make_float4(c0.x, c0.y, c0.z, 0.f);
+                            w.sh_c1[slot] = make_float4(c1.x, c1.y, c1.z, 0.f);
                             w.sh_t[slot] = make_float4(T.x, T.y, T.z, 0.f);
-                            push_sh = true;
+                            w.sh_vis[slot] = 0u;
+                            push_sh0 = r0;
+                            push_sh1 = r1;
                         }
                     }
                 }
@@ -365,52 +410,66 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                     }
                 }
                 lo = make_float4(Lo.x, Lo.y, Lo.z, lo.w);
-                w.state[slot] = alive ? PS_ACTIVE : PS_DONE;
+                w.state[slot] = (alive ? PS_ACTIVE : PS_DONE) | (push_sh0 || push_sh1 ? PS_PENDING : 0u);
                 push_ext = alive;
             }
             w.lo[slot] = lo;
         }
         warp_push(push_ext, slot, qout, cout);
-        warp_push(push_sh, slot, w.q_shadow, &w.ctr[C_SHADOW]);
+        warp_push(push_sh0, slot << 1, w.q_shadow, &w.ctr[C_SHADOW]);
+        warp_push(push_sh1, (slot << 1) | 1u, w.q_shadow, &w.ctr[C_SHADOW]);
     }
 }
 
 // ------------------------------------------------------------------ shadow
+// Occlusion of the next-event rays (entries slot << 1 | ray); lanes are refilled as in
+// k_extend. An unoccluded ray sets its bit in sh_vis; the next regen adds the light.
 __global__ void k_shadow(WfPool w) {
     const uint32_t n = w.ctr[C_SHADOW];
-    uint32_t nrays = 0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) w.rays[1] += n;
+    int stack[kTraversalStack];
+    TraceState<true> ts;
+    const BvhNode* nodes = nullptr;
+    const BvhTri* tris = nullptr;
+    uint32_t entry = 0;
+    bool has = false, exhausted = false;
     while (true) {
-        const uint32_t b = warp_fetch(&w.ctr[C_CUR_SHADOW]);
-        if (b >= n) break;
-        const uint32_t k = b + lane_id();
-        if (k < n) {
-            const uint32_t slot = w.q_shadow[k];
-            const WfScene& S = w.scenes[w.id[slot].x];
-            const float4 p = w.sh_p[slot], c0 = w.sh_c0[slot], c1 = w.sh_c1[slot];
-            const float3 P = mk(p.x, p.y, p.z);
-            TraceWork work;
-            float3 res = mk(0.f, 0.f, 0.f);
-            nrays += (c0.w != 0.f) + (c1.w != 0.f);
-            if (c0.w != 0.f) {
-                const float4 d = w.sh_d0[slot];
-                if (!bvh_occluded(S.sc.nodes, S.sc.tris, P, mk(d.x, d.y, d.z), kRayBias, d.w, work))
-                    res += mk(c0.x, c0.y, c0.z);
+        const bool need = !has && !exhausted;
+        const uint32_t m = __ballot_sync(0xffffffffu, need);
+        const uint32_t act = __ballot_sync(0xffffffffu, has);
+        if (m && (__popc(m) >= kRefill || act == 0)) {
+            const int leader = __ffs(m) - 1;
+            uint32_t b = 0;
+            if ((int)lane_id() == leader) b = atomicAdd(&w.ctr[C_CUR_SHADOW], (uint32_t)__popc(m));
+            b = __shfl_sync(0xffffffffu, b, leader);
+            if (need) {
+                const uint32_t k = b + __popc(m & lanemask_lt());
+                if (k < n) {
+                    entry = w.q_shadow[k];
+                    const uint32_t slot = entry >> 1;
+                    const WfScene& S = w.scenes[w.id[slot].x];
+                    nodes = S.sc.nodes;
+                    tris = S.sc.tris;
+                    const float4 p = w.sh_p[slot];
+                    const float4 d = (entry & 1u) ? w.sh_d1[slot] : w.sh_d0[slot];
+                    ts.begin(mk(p.x, p.y, p.z), mk(d.x, d.y, d.z), kRayBias, d.w);
+                    has = true;
+                } else {
+                    exhausted = true;
+                }
             }
-            if (c1.w != 0.f) {
-                const float4 d = w.sh_d1[slot];
-                if (!bvh_occluded(S.sc.nodes, S.sc.tris, P, mk(d.x, d.y, d.z), kRayBias, d.w, work))
-                    res += mk(c1.x, c1.y, c1.z);
+        }
+        if (__ballot_sync(0xffffffffu, has || !exhausted) == 0) break;
+        if (has) {
+            for (int k = 0; k < kSteps; ++k) {
+                if (ts.step(nodes, tris, stack)) {
+                    if (!ts.hit_any) atomicOr(&w.sh_vis[entry >> 1], 1u << (entry & 1u));
+                    has = false;
+                    break;
+                }
             }
-            const float4 t = w.sh_t[slot];
-            float4 lo = w.lo[slot];
-            const float3 add = (res * p.w) * mk(t.x, t.y, t.z);
-            lo.x += add.x; lo.y += add.y; lo.z += add.z;
-            w.lo[slot] = lo;
         }
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) nrays += __shfl_xor_sync(0xffffffffu, nrays, o);
-    if (lane_id() == 0 && nrays) atomicAdd(&w.rays[1], (unsigned long long)nrays);
 }
 
 // ------------------------------------------------------------------ resolve
@@ -475,7 +534,7 @@ struct WfRun {
         cfg = c;
         stream = s;
         const size_t P = c.pool;
-        const size_t bytes = P * (11 * sizeof(float4) + sizeof(uint4) + 5 * sizeof(uint32_t)) + 18 * 256 +
+        const size_t bytes = P * (11 * sizeof(float4) + sizeof(uint4) + 7 * sizeof(uint32_t)) + 19 * 256 +
                              kCounters * sizeof(uint32_t) + 2 * sizeof(unsigned long long);
         cudaError_t e = cudaMalloc(&mem, bytes);
         if (e != cudaSuccess) return e;
@@ -488,7 +547,8 @@ struct WfRun {
         w.q_ext0 = (uint32_t*)take(P * 4);
         w.q_ext1 = (uint32_t*)take(P * 4);
         w.q_sort = (uint32_t*)take(P * 4);
-        w.q_shadow = (uint32_t*)take(P * 4);
+        w.q_shadow = (uint32_t*)take(2 * P * 4);   // up to two next-event rays per slot
+        w.sh_vis = (uint32_t*)take(P * 4);
         w.ctr = (uint32_t*)take(kCounters * 4);
         w.rays = (unsigned long long*)take(2 * sizeof(unsigned long long));
         if ((size_t)(p - (char*)mem) > bytes) return cudaErrorMemoryAllocation;

@@ -243,14 +243,17 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        kernel_ms, launches, stats = 0.0, 0, None
+        kernel_ms, launches, stats, host = 0.0, 0, None, []
         e0.record(stream)
         for _ in range(steps):
+            t0 = time.perf_counter()
             res = frame(modes[mode])
+            host.append((time.perf_counter() - t0) * 1000.0)
             kernel_ms += res.stats["kernel_ms"]
             launches += res.stats["launches"]
             stats = res.stats
         e1.record(stream)
+        stats = dict(stats, host_ms_per_call=host)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if dist:
@@ -354,6 +357,7 @@ def main():
                            "renderer": head, "l2": "inputs larger than L2 (BVH+triangles > 126 MB); no flush",
                            "multi_gpu": "each rank renders the full frame with its own sample indices"},
                 "rays_per_s": world * rays_step / (ms_step / 1000.0), "kernel_ms_per_step": kms_step,
+                "host_ms_per_call": st.get("host_ms_per_call"),
                 "bvh_build_s": build_s, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
                 "e2e": e2e, "clocks": clk}
         line.update(other)
