@@ -9,6 +9,7 @@
 // The triangle test is the exact FP32 Moller-Trumbore of tri_intersect, so the
 // closest prim equals a brute-force scan's whenever the minimum is unique.
 #pragma once
+#include <climits>
 #include "aur_bvh.cuh"
 #include "aur_shading.cuh"
 
@@ -134,7 +135,71 @@ struct TraceState {
         box_tmax = tbest * 1.00000095f;
         bu = bv = 0.f;
         node = 0; sp = 0; best = -1;
+        leaf = kNone;
         hit_any = false;
+    }
+
+    // One round of "while-while" traversal with speculative leaf postponing (Aila &
+    // Laine, "Understanding the Efficiency of Ray Traversal on GPUs", HPG 2009): the
+    // interior loop runs until every lane of the warp holds a leaf (or has finished),
+    // lanes that already hold one keep descending speculatively, then all lanes test
+    // their leaf's triangles together. `live` marks lanes that have a ray; all 32
+    // lanes of the warp must call round(). Returns true when this lane's ray is done.
+    int leaf;        // postponed leaf reference, kNone if none
+    static constexpr int kNone = INT_MIN;
+
+    __device__ __forceinline__ bool round(const BvhNode* __restrict__ nodes, const BvhTri* __restrict__ tris,
+                                          int* stack, bool live) {
+        bool finished = !live;
+        if (live && leaf == kNone && node == kNone) finished = true;
+        // interior phase
+        while (true) {
+            bool searching = false;
+            if (!finished && node != kNone && node >= 0) {
+                const float4 a = __ldg(&nodes[node].a);
+                const float4 b = __ldg(&nodes[node].b);
+                const float4 c = __ldg(&nodes[node].c);
+                const float4 e = __ldg(&nodes[node].d);
+                float t0, t1;
+                const bool h0 = slab(a.x, a.y, a.z, a.w, c.x, c.y, id, ood, box_tmin, box_tmax, &t0);
+                const bool h1 = slab(b.x, b.y, b.z, b.w, c.z, c.w, id, ood, box_tmin, box_tmax, &t1);
+                const int r0 = __float_as_int(e.x), r1 = __float_as_int(e.y);
+                if (h0 && h1) {
+                    const bool first0 = t0 <= t1;
+                    if (sp < kTraversalStack) stack[sp++] = first0 ? r1 : r0;   // depth <= 63 is checked at build
+                    node = first0 ? r0 : r1;
+                } else if (h0) node = r0;
+                else if (h1) node = r1;
+                else node = sp > 0 ? stack[--sp] : kNone;
+            }
+            if (!finished && node != kNone && node < 0 && leaf == kNone) {   // postpone this leaf
+                leaf = node;
+                node = sp > 0 ? stack[--sp] : kNone;
+            }
+            if (!finished) searching = leaf == kNone && node != kNone;   // still looking for a leaf
+            if (!__any_sync(0xffffffffu, searching)) break;
+        }
+        // leaf phase
+        if (!finished && leaf != kNone) {
+            const int packed = ~leaf;
+            const int start = packed >> 5, end = start + (packed & 31);
+            leaf = kNone;
+            for (int k = start; k < end; ++k) {
+                const float4 p = __ldg(&tris[k].p1);
+                const float4 e1 = __ldg(&tris[k].e1);
+                const float4 e2 = __ldg(&tris[k].e2);
+                float t, u, v;
+                if (tri_intersect(mk(p.x, p.y, p.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), o, d, mint, tbest,
+                                  &t, &u, &v)) {
+                    if (kAnyHit) { hit_any = true; return true; }
+                    tbest = t; bu = u; bv = v;
+                    best = __float_as_int(p.w);
+                    box_tmax = tbest * 1.00000095f;
+                }
+            }
+        }
+        if (finished) return live;
+        return leaf == kNone && node == kNone;
     }
 
     __device__ __forceinline__ bool step(const BvhNode* __restrict__ nodes, const BvhTri* __restrict__ tris,

@@ -31,10 +31,10 @@ namespace aur {
 namespace {
 
 enum : uint32_t { PS_EMPTY = 0, PS_ACTIVE = 1, PS_DONE = 2, PS_MASK = 3, PS_PENDING = 4 };
-// lane refill: a warp takes new rays once this many lanes are idle, and every lane
-// advances its traversal by up to kSteps nodes/leaves between refill checks
+// lane refill: a warp takes new rays once this many lanes are idle, and runs kRounds
+// traversal rounds (interior phase + leaf phase) between refill checks
 constexpr int kRefill = 16;
-constexpr int kSteps = 16;
+constexpr int kRounds = 2;
 enum : int { B_MISS = 0, B_MATTE = 1, B_KELEMEN = 2, B_CT = 3, B_METAL = 4, B_CONST = 5, kBuckets = 6 };
 // counters
 enum : int {
@@ -227,10 +227,10 @@ __global__ void k_extend(WfPool w, int in_q) {
         }
         if (__ballot_sync(0xffffffffu, has || !exhausted) == 0) break;
         bool done = false;
-        if (has) {
-            for (int k = 0; k < kSteps; ++k)
-                if (ts.step(nodes, tris, stack)) { done = true; break; }
+        for (int k = 0; k < kRounds; ++k) {          // all lanes take part in every round
+            if (ts.round(nodes, tris, stack, has && !done)) done = true;
         }
+        done = done && has;
         int bucket = -1;
         if (done) {
             w.hit[slot] = make_float4(ts.tbest, ts.bu, ts.bv, __int_as_float(ts.best));
@@ -460,14 +460,13 @@ __global__ void k_shadow(WfPool w) {
             }
         }
         if (__ballot_sync(0xffffffffu, has || !exhausted) == 0) break;
-        if (has) {
-            for (int k = 0; k < kSteps; ++k) {
-                if (ts.step(nodes, tris, stack)) {
-                    if (!ts.hit_any) atomicOr(&w.sh_vis[entry >> 1], 1u << (entry & 1u));
-                    has = false;
-                    break;
-                }
-            }
+        bool done = false;
+        for (int k = 0; k < kRounds; ++k) {
+            if (ts.round(nodes, tris, stack, has && !done)) done = true;
+        }
+        if (done && has) {
+            if (!ts.hit_any) atomicOr(&w.sh_vis[entry >> 1], 1u << (entry & 1u));
+            has = false;
         }
     }
 }
@@ -520,6 +519,8 @@ struct WfRun {
     int cap_scenes = 0;
     float4* samples = nullptr;                 // per-sample buffer, grown on demand
     size_t samples_bytes = 0;
+    float4* acc = nullptr;                     // per-pixel compensated sums, grown on demand
+    size_t acc_bytes = 0;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
     int grid_regen = 0, grid_ext = 0, grid_shade = 0, grid_shadow = 0, grid_sort = 0;
@@ -649,7 +650,20 @@ struct WfRun {
         return e;
     }
 
+    cudaError_t ensure_acc(size_t bytes) {
+        if (bytes <= acc_bytes) return cudaSuccess;
+        if (acc) cudaFree(acc);
+        acc = nullptr;
+        acc_bytes = 0;
+        cudaError_t e = cudaMalloc(&acc, bytes);
+        if (e == cudaSuccess) acc_bytes = bytes;
+        return e;
+    }
+
     void release() {
+        if (acc) cudaFree(acc);
+        acc = nullptr;
+        acc_bytes = 0;
         if (exec) cudaGraphExecDestroy(exec);
         if (mem) cudaFree(mem);
         if (d_scenes) cudaFree(d_scenes);
@@ -812,6 +826,15 @@ static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, c
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)max_spp, budget / std::max<size_t>(per_sample, 1)));
     e = run.ensure_samples(per_sample * chunk);
     float4* samples = run.samples;
+    if (e == cudaSuccess) e = run.ensure_acc(2 * per_sample);   // two float4 per pixel
+    {
+        size_t off = 0;
+        for (auto& it : items) {
+            it.acc_s = run.acc + off;
+            it.acc_c = run.acc + off + it.npix;
+            off += 2 * (size_t)it.npix;
+        }
+    }
     for (auto& it : items) {
         if (e == cudaSuccess) e = cudaMemsetAsync(it.acc_s, 0, sizeof(float4) * it.npix, s);
         if (e == cudaSuccess) e = cudaMemsetAsync(it.acc_c, 0, sizeof(float4) * it.npix, s);
@@ -909,12 +932,10 @@ aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film
     if ((uint64_t)npix * o->spp >= (1ull << 31)) return fail(AUR_ERR_INVALID_ARG, "aur_render: more than 2^31 paths");
     DevOut fo;
     cudaError_t e = fo.init(film, sizeof(float4) * npix, 16, s);
-    float4 *acc = nullptr;
-    if (e == cudaSuccess) e = cudaMallocAsync(&acc, sizeof(float4) * 2 * npix, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // buffers allocated on the caller's stream
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // film staging allocated on the caller's stream
     if (e != cudaSuccess) return cuda_fail(e, "aur_render(wavefront)");
     std::vector<BatchItem> items(1);
-    items[0] = {sc, p, npix, acc, acc + npix};
+    items[0] = {sc, p, npix, nullptr, nullptr};
     if (wants_tuning(o)) {
         if (!sc->wf_tuned) {
             // A scene of the same shape (triangles, materials, lights, resolution, spp,
@@ -927,7 +948,7 @@ aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film
             auto it = sc->ctx->wf_scene_tuned.find(sig);
             if (it == sc->ctx->wf_scene_tuned.end()) {
                 WfConfig t;
-                if ((st = autotune(sc->ctx, items, &t)) != AUR_OK) { cudaFreeAsync(acc, s); return st; }
+                if ((st = autotune(sc->ctx, items, &t)) != AUR_OK) return st;
                 it = sc->ctx->wf_scene_tuned.emplace(sig, std::array<int, 3>{(int)t.pool, t.block, t.sort}).first;
             }
             sc->wf_pool = it->second[0]; sc->wf_block = it->second[1]; sc->wf_sort = it->second[2];
@@ -943,8 +964,6 @@ aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) st = cuda_fail(e, "aur_render(wavefront download)");
     }
-    cudaFreeAsync(acc, s);
-    cudaStreamSynchronize(s);
     return st;
 }
 
@@ -980,8 +999,6 @@ extern "C" aur_status aur_render_batch(aur_scene* const* scenes, const aur_rende
     for (uint32_t i = 0; i < n && e == cudaSuccess; ++i) {
         e = outs[i].init(films[i], sizeof(float4) * items[i].npix, 16, s);
         fl[i] = (float4*)outs[i].ptr;
-        if (e == cudaSuccess) e = cudaMallocAsync(&items[i].acc_s, sizeof(float4) * 2 * items[i].npix, s);
-        items[i].acc_c = items[i].acc_s + items[i].npix;
     }
     float ms = 0.f;
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -1002,7 +1019,6 @@ extern "C" aur_status aur_render_batch(aur_scene* const* scenes, const aur_rende
         e = outs[i].finish();
         if (e != cudaSuccess) st = cuda_fail(e, "aur_render_batch(download)");
     }
-    for (uint32_t i = 0; i < n; ++i) if (items[i].acc_s) cudaFreeAsync(items[i].acc_s, s);
     cudaStreamSynchronize(s);
     return st;
 }
