@@ -114,6 +114,22 @@ __device__ __forceinline__ bool bvh_occluded(const BvhNode* nodes, const BvhTri*
 
 namespace aur {
 
+// Traversal stack of one thread: the first kSharedDepth entries live in shared
+// memory laid out [depth][thread] (consecutive threads hit consecutive banks at
+// any mix of depths, one wavefront per warp access), deeper entries in local memory.
+constexpr int kSharedDepth = 24;
+struct LaneStack {
+    int* col;                       // &s_stack[threadIdx.x]
+    int stride;                     // blockDim.x
+    int deep[kTraversalStack - kSharedDepth];
+    __device__ __forceinline__ void set(int i, int v) {
+        if (i < kSharedDepth) col[i * stride] = v; else deep[i - kSharedDepth] = v;
+    }
+    __device__ __forceinline__ int get(int i) const {
+        return i < kSharedDepth ? col[i * stride] : deep[i - kSharedDepth];
+    }
+};
+
 // Resumable traversal of one ray, for persistent kernels whose lanes take a new
 // ray as soon as theirs finishes (lane refill). Same visiting order, slack and
 // exact triangle test as bvh_trace; step() advances one interior node or one
@@ -149,7 +165,7 @@ struct TraceState {
     static constexpr int kNone = INT_MIN;
 
     __device__ __forceinline__ bool round(const BvhNode* __restrict__ nodes, const BvhTri* __restrict__ tris,
-                                          int* stack, bool live) {
+                                          LaneStack& stack, bool live) {
         bool finished = !live;
         if (live && leaf == kNone && node == kNone) finished = true;
         // interior phase
@@ -166,15 +182,15 @@ struct TraceState {
                 const int r0 = __float_as_int(e.x), r1 = __float_as_int(e.y);
                 if (h0 && h1) {
                     const bool first0 = t0 <= t1;
-                    if (sp < kTraversalStack) stack[sp++] = first0 ? r1 : r0;   // depth <= 63 is checked at build
+                    if (sp < kTraversalStack) stack.set(sp++, first0 ? r1 : r0);   // depth <= 63 is checked at build
                     node = first0 ? r0 : r1;
                 } else if (h0) node = r0;
                 else if (h1) node = r1;
-                else node = sp > 0 ? stack[--sp] : kNone;
+                else node = sp > 0 ? stack.get(--sp) : kNone;
             }
             if (!finished && node != kNone && node < 0 && leaf == kNone) {   // postpone this leaf
                 leaf = node;
-                node = sp > 0 ? stack[--sp] : kNone;
+                node = sp > 0 ? stack.get(--sp) : kNone;
             }
             if (!finished) searching = leaf == kNone && node != kNone;   // still looking for a leaf
             if (!__any_sync(0xffffffffu, searching)) break;

@@ -35,6 +35,10 @@ enum : uint32_t { PS_EMPTY = 0, PS_ACTIVE = 1, PS_DONE = 2, PS_MASK = 3, PS_PEND
 // traversal rounds (interior phase + leaf phase) between refill checks
 constexpr int kRefill = 16;
 constexpr int kRounds = 2;
+// resident 256-thread blocks per SM the traversal kernels are compiled for (register cap)
+#ifndef AUR_TRAV_MINB
+#define AUR_TRAV_MINB 4
+#endif
 enum : int { B_MISS = 0, B_MATTE = 1, B_KELEMEN = 2, B_CT = 3, B_METAL = 4, B_CONST = 5, kBuckets = 6 };
 // counters
 enum : int {
@@ -180,7 +184,7 @@ __device__ __forceinline__ int bucket_of(const ShadeScene& sh, int prim) {
 // finished lanes are refilled from the queue (one atomic per warp) while the
 // others continue, so a warp is not held up by its slowest ray.
 template <bool kSort>
-__global__ void k_extend(WfPool w, int in_q) {
+__global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_q) {
     const uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
     const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
     // Outputs of the later stages start empty. Only counters that no block of
@@ -194,7 +198,10 @@ __global__ void k_extend(WfPool w, int in_q) {
         w.ctr[C_CUR_SORT] = 0;
         w.rays[0] += n;
     }
-    int stack[kTraversalStack];
+    extern __shared__ int s_stack[];
+    LaneStack stack;
+    stack.col = s_stack + threadIdx.x;
+    stack.stride = blockDim.x;
     TraceState<false> ts;
     const BvhNode* nodes = nullptr;
     const BvhTri* tris = nullptr;
@@ -424,10 +431,13 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
 // ------------------------------------------------------------------ shadow
 // Occlusion of the next-event rays (entries slot << 1 | ray); lanes are refilled as in
 // k_extend. An unoccluded ray sets its bit in sh_vis; the next regen adds the light.
-__global__ void k_shadow(WfPool w) {
+__global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_shadow(WfPool w) {
     const uint32_t n = w.ctr[C_SHADOW];
     if (blockIdx.x == 0 && threadIdx.x == 0) w.rays[1] += n;
-    int stack[kTraversalStack];
+    extern __shared__ int s_stack[];
+    LaneStack stack;
+    stack.col = s_stack + threadIdx.x;
+    stack.stride = blockDim.x;
     TraceState<true> ts;
     const BvhNode* nodes = nullptr;
     const BvhTri* tris = nullptr;
@@ -524,6 +534,7 @@ struct WfRun {
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
     int grid_regen = 0, grid_ext = 0, grid_shade = 0, grid_shadow = 0, grid_sort = 0;
+    size_t stack_smem = 0;                     // shared traversal stack of one block
     uint32_t* h_ctr = nullptr;   // pinned
     static constexpr int kItersPerGraph = 8;
     static constexpr int kStages = 5;          // regen, extend, sort, shade, shadow
@@ -565,15 +576,16 @@ struct WfRun {
         int dev = 0, sms = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        auto persist = [&](const void* fn) {
+        stack_smem = (size_t)kSharedDepth * c.block * sizeof(int);
+        auto persist = [&](const void* fn, size_t smem) {
             int nb = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, c.block, 0);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, c.block, smem);
             return std::max(1, nb) * sms;
         };
-        grid_ext = persist(c.sort ? (const void*)k_extend<true> : (const void*)k_extend<false>);
-        grid_shade = persist((const void*)k_shade);
-        grid_shadow = persist((const void*)k_shadow);
-        grid_sort = persist((const void*)k_sort_scatter);
+        grid_ext = persist(c.sort ? (const void*)k_extend<true> : (const void*)k_extend<false>, stack_smem);
+        grid_shade = persist((const void*)k_shade, 0);
+        grid_shadow = persist((const void*)k_shadow, stack_smem);
+        grid_sort = persist((const void*)k_sort_scatter, 0);
         grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 16);
         return cudaSuccess;
     }
@@ -584,14 +596,14 @@ struct WfRun {
         cudaEvent_t* e = &ev[it * kStages + 1];
         k_regen<<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[0], stream, cudaEventRecordExternal);
-        if (cfg.sort) k_extend<true><<<grid_ext, cfg.block, 0, stream>>>(w, in_q);
-        else k_extend<false><<<grid_ext, cfg.block, 0, stream>>>(w, in_q);
+        if (cfg.sort) k_extend<true><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
+        else k_extend<false><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[1], stream, cudaEventRecordExternal);
         if (cfg.sort) k_sort_scatter<<<grid_sort, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[2], stream, cudaEventRecordExternal);
         k_shade<<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
         cudaEventRecordWithFlags(e[3], stream, cudaEventRecordExternal);
-        k_shadow<<<grid_shadow, cfg.block, 0, stream>>>(w);
+        k_shadow<<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
         cudaEventRecordWithFlags(e[4], stream, cudaEventRecordExternal);
     }
 
