@@ -135,6 +135,46 @@ def cpu_baseline(data, tables, budget_s=15.0):
     return paths / dt, f"{W}x{rows} rows at y={y0} x {r['spp']} spp ({paths} paths, {dt:.1f} s)", cores, build_s
 
 
+def adjoint_ratio(ab, _abi, torch, ctx, stream, steps=2, warmup=1):
+    """Device time of the path-replay adjoint over the device time of the forward render on
+    the differentiable workload (256x256, 256 spp, depth 6, 64x64 RGB texture, 16 materials).
+    dL/dfilm is a resident device tensor; the parameter gradients come back to host arrays."""
+    from aurora_b200 import scenes
+    data = scenes.texture_scene()
+    sc = ab.Scene(ctx, data)
+    H, W = data.height, data.width
+    spp, depth = data.render["spp"], data.render["max_depth"]
+    film = torch.empty((H, W, 4), dtype=torch.float32, device="cuda")
+    g = torch.Generator(device="cpu").manual_seed(8)
+    dfilm = torch.randn((H, W, 4), generator=g).to("cuda")
+    gm = np.zeros((sc.nmat, 4), np.float32)
+    gt = np.zeros(max(sc.ntexel, 1), np.float32)
+
+    def dev_ms(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    def fwd(mode):
+        return lambda: sc.render(ab.render_opts(spp, depth, depth, data.render["seed"], mode=mode), out=film)
+
+    f_wf = dev_ms(fwd(_abi.RENDER_WAVEFRONT))
+    f_plain = dev_ms(fwd(_abi.RENDER_PLAIN))
+    adj = dev_ms(lambda: sc.adjoint(ab.render_opts(spp, depth, depth, data.render["seed"]), dfilm, gm, gt))
+    sc.close()
+    return {"workload": f"texture {data.ntri} tris {W}x{H} {spp}spp depth {depth}, 16 materials + 64x64x3 texels",
+            "forward_ms": f_wf, "forward_plain_ms": f_plain, "adjoint_ms": adj, "ratio": adj / f_wf,
+            "ratio_vs_plain": adj / f_plain,
+            "note": "forward = wavefront render (the autograd forward); adjoint = record + replay passes"}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -341,6 +381,8 @@ def main():
                "d2h_bytes_per_step": int(host_film.nbytes), "ms_per_step": dt * 1000,
                "includes": "scene upload + device BVH build + render + film download"}
 
+    adj = None if args.small else adjoint_ratio(ab, _abi, torch, ctx, stream)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         tables = np.stack([ctx.kelemen_table(k / 20.0) for k in range(21)])
@@ -359,7 +401,7 @@ def main():
                 "rays_per_s": world * rays_step / (ms_step / 1000.0), "kernel_ms_per_step": kms_step,
                 "host_ms_per_call": st.get("host_ms_per_call"),
                 "bvh_build_s": build_s, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "e2e": e2e, "clocks": clk}
+                "e2e": e2e, "clocks": clk, "adjoint_forward": adj}
         line.update(other)
         print(json.dumps(line), flush=True)
     scene.close()

@@ -16,6 +16,8 @@
 //     RenderableTriangle Moller-Trumbore test (renderableTriangle.cpp:68-98);
 //   * the film is an FP64 running sum (the reference keeps half precision);
 //   * the unshaded closest-hit ray after the last vertex is not traced.
+// The adjoint restatement (oracle_adjoint) has no reference counterpart: it is the
+// FP64 forward-mode derivative of this file's own estimator.
 // Parity pinning: the reference ships no tests, golden vectors or fixtures and
 // cannot be built here (Embree 1.x, TBB 4.1, OpenEXR 1.7, jsoncpp absent), so
 // this restatement is pinned by its line-by-line correspondence and by the
@@ -157,7 +159,7 @@ struct Light {
     int type; float xScale, yScale, radius; Point pCam[4]; Vector lightN; Color le; Point center; float m[16];
     Point tri[2][3];
 };
-struct Tex { int w, h; const float* px; };
+struct Tex { int w, h; const float* px; size_t offset; };   // offset: first float in the texel array
 
 struct BvhNode { float lo[3], hi[3]; int left, right, start, count; };   // leaf if count > 0
 
@@ -477,8 +479,7 @@ static float brdfPdf(const BrdfState& b, const Vector& L, const Vector& V, const
 }
 
 // ------------------------------------------------------------ textures (texture2DShader.h:28-31, texture2D.cpp:48-72)
-static Color texRead(const Scene& sc, int tex, float u, float v) {
-    const Tex& t = sc.texs[tex];
+static int texelOf(const Tex& t, float u, float v) {     // nearest texel (filter 0)
     float s = u - afloor(u);
     float tt = 1.f - (v - afloor(v));
     int x = afloor(s * t.w);
@@ -487,7 +488,11 @@ static Color texRead(const Scene& sc, int tex, float u, float v) {
     if (x == t.w) x -= 1;
     x = std::max(0, std::min(x, t.w - 1));
     y = std::max(0, std::min(y, t.h - 1));
-    const float* p = t.px + 3 * (y * t.w + x);
+    return y * t.w + x;
+}
+static Color texRead(const Scene& sc, int tex, float u, float v) {
+    const Tex& t = sc.texs[tex];
+    const float* p = t.px + 3 * texelOf(t, u, v);
     return Color(p[0], p[1], p[2]);
 }
 
@@ -668,8 +673,35 @@ static LocalGeometry hitGeometry(const Scene& sc, const Ray& ray, int prim, floa
     return lg;
 }
 
+// Derivatives of one vertex's next-event estimate D (adjoint only, FP64): per channel
+// dD_c/d(albedo_c) of a Lambert lobe and dD_c/d(roughness) of a Cook-Torrance lobe.
+// Sampling pdfs and MIS weights are constants of the derivative.
+struct DirectGrad { double dAlbedo[3] = {0, 0, 0}, dRough[3] = {0, 0, 0}; };
+
+// d ln D / d roughness of the Beckmann term at the half vector (ndoth), FP64:
+// D = exp(-tan^2/r^2) / (r^2 pi cos^3), tan^2 = (1 - cos^2) / cos^2.
+static double dlnBeckmann(double r, double ndoth) {
+    const double c2 = ndoth * ndoth;
+    const double tan2 = (1.0 - c2) / c2;
+    return 2.0 * tan2 / (r * r * r) - 2.0 / r;
+}
+// the same for a sampled direction (cookTorrance.cpp:47-99): ctD floors r^2 at 0.001 and
+// the sample clamps D at 1000, where the sample's colour no longer depends on roughness
+static double dlnBeckmannSampled(const BrdfState& b, const Vector& L, const Vector& V, const Vector& N) {
+    const double hx = (double)L.x + V.x, hy = (double)L.y + V.y, hz = (double)L.z + V.z;
+    const double hl = std::sqrt(hx * hx + hy * hy + hz * hz);
+    const double ndoth = (hx * N.x + hy * N.y + hz * N.z) / hl;
+    const double r = b.roughness;
+    if (r * r <= 0.001) return 0.0;
+    const double c2 = ndoth * ndoth;
+    const double tan2 = ndoth > 0.999 ? 0.0 : (1.0 - c2) / c2;
+    const double D = std::exp(-tan2 / (r * r)) / (r * r * M_PI * c2 * ndoth);
+    if (D >= 1000.0) return 0.0;
+    return 2.0 * tan2 / (r * r * r) - 2.0 / r;
+}
+
 static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const BrdfState& brdf, const Rng& rng, int vtx,
-                             Counts& cnt) {
+                             Counts& cnt, DirectGrad* grad = nullptr) {
     Color result(0.f);
     int numLights = 0;
     std::vector<int> idx;
@@ -684,8 +716,13 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
         float costheta = dot(lg.Nn, ls.ray.direction);
         if (costheta >= 0. && ls.pdf > 0.) {
             ++cnt.shadow;
-            if (!sceneOccluded(sc, ls.ray))
+            if (!sceneOccluded(sc, ls.ray)) {
                 result += ls.color * brdfEval(brdf, ls.ray.direction, lg.Vn, lg.Nn) * costheta / ls.pdf;
+                if (grad && dot(ls.ray.direction, lg.Nn) > 0.) {       // eval = albedo / pi
+                    const double k = (double)costheta / ls.pdf / M_PI;
+                    grad->dAlbedo[0] += ls.color.r * k; grad->dAlbedo[1] += ls.color.g * k; grad->dAlbedo[2] += ls.color.b * k;
+                }
+            }
         }
     } else if (brdf.type == SpecBrdf) {                                   // integrateDirectMIS :56-98
         Sample3D ls = lightGenerateSample(light, lg.P, lx, ly);
@@ -696,7 +733,15 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
                 ++cnt.shadow;
                 if (!sceneOccluded(sc, ls.ray)) {
                     float weight = PowerHeuristic(1, ls.pdf, 1, bp);
-                    result += ls.color * weight * brdfEval(brdf, ls.ray.direction, lg.Vn, lg.Nn) * costheta / ls.pdf;
+                    Color c0 = ls.color * weight * brdfEval(brdf, ls.ray.direction, lg.Vn, lg.Nn) * costheta / ls.pdf;
+                    result += c0;
+                    if (grad) {
+                        const Vector& L = ls.ray.direction;
+                        const double hx = (double)L.x + lg.Vn.x, hy = (double)L.y + lg.Vn.y, hz = (double)L.z + lg.Vn.z;
+                        const double ndoth = (hx * lg.Nn.x + hy * lg.Nn.y + hz * lg.Nn.z) / std::sqrt(hx * hx + hy * hy + hz * hz);
+                        const double g = dlnBeckmann(brdf.roughness, ndoth);
+                        grad->dRough[0] += c0.r * g; grad->dRough[1] += c0.g * g; grad->dRough[2] += c0.b * g;
+                    }
                 }
             }
         }
@@ -709,12 +754,19 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
                 ++cnt.shadow;
                 if (!sceneOccluded(sc, bs.ray)) {
                     float weight = PowerHeuristic(1, bs.pdf, 1, lp);
-                    result += bs.color * weight * light.le * costheta / bs.pdf;
+                    Color c1 = bs.color * weight * light.le * costheta / bs.pdf;
+                    result += c1;
+                    if (grad) {
+                        const double g = dlnBeckmannSampled(brdf, bs.ray.direction, lg.Vn, lg.Nn);
+                        grad->dRough[0] += c1.r * g; grad->dRough[1] += c1.g * g; grad->dRough[2] += c1.b * g;
+                    }
                 }
             }
         }
     }
     result *= (float)numLights;
+    if (grad)
+        for (int c = 0; c < 3; ++c) { grad->dAlbedo[c] *= numLights; grad->dRough[c] *= numLights; }
     return result;
 }
 
@@ -763,6 +815,156 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
     if (!std::isfinite(Lo.r) || !std::isfinite(Lo.g) || !std::isfinite(Lo.b)) return Color(0.f);
     while (Lo.r > FIREFLY || Lo.g > FIREFLY || Lo.b > FIREFLY) Lo *= 0.2f;
     return Lo;
+}
+
+// ------------------------------------------------------------ adjoint restatement (FP64, forward mode)
+// Derivative of integrateCameraSample's estimator with the sampling decisions held
+// fixed (pdfs, MIS weights, lobe choice, roulette and the firefly factor are constants),
+// carried FORWARD along the path in double:
+//   L = sum_k T_k D_k,  T_{k+1} = T_k w_k / q_k
+//   dT_{k+1} = (dT_k w_k + T_k dw_k) / q_k,   dL += dT_k D_k + T_k dD_k
+// plus the score d ln P(lobe_k)/dr of Kelemen's lobe choice on every term from vertex k
+// on. (The product evaluates the same quantity in reverse, by path replay.)
+// Parameter vector: per material m (diffuse r, g, b, roughness) at 4m..4m+3, then the
+// texel floats at 4 nmat + i.
+struct ParamRef { long base = -1; bool perChannel = false; double chain = 1.0; };
+
+static ParamRef paramOf(const Scene& sc, int matId, const BrdfState& b, const LocalGeometry& lg, bool mattePath,
+                        float lobeU) {
+    ParamRef p;
+    const Mat& m = sc.mats[matId];
+    if (b.type == MatteBrdf) {                       // albedo (matte, Kelemen's diffuse lobe)
+        if (m.type != AUR_MAT_MATTE && m.type != AUR_MAT_KELEMEN) return p;
+        p.perChannel = true;
+        if (m.diffTex >= 0) {
+            const Tex& t = sc.texs[m.diffTex];
+            p.base = 4 * (long)sc.mats.size() + (long)t.offset + 3 * texelOf(t, lg.su, lg.sv);
+        } else {
+            p.base = 4 * matId;
+        }
+        return p;
+    }
+    if (b.type == SpecBrdf && m.roughTex < 0 &&
+        (m.type == AUR_MAT_KELEMEN || m.type == AUR_MAT_COOKTORRANCE || (m.type == AUR_MAT_METAL && lobeU > m.mix))) {
+        p.base = 4 * matId + 3;                      // roughness; blurred on matte paths (kelemenMaterial.cpp:232-234)
+        p.chain = mattePath ? 1.0 - CAUSTIC_BLUR : 1.0;
+    }
+    return p;
+}
+
+// d ln P(chosen lobe) / d roughness of Kelemen's choice (kelemenMaterial.cpp:236-253):
+// P(spec) = A(cos, r_eff) clamped to [0, 1]; getAlbedo is linear in r * 31 between
+// column ra and column rb (rb = 31: the reference's max(ra + 1, 31)).
+static double kelemenScore(const Scene& sc, const Mat& m, const LocalGeometry& lg, const BrdfState& b, bool mattePath) {
+    if (m.type != AUR_MAT_KELEMEN || m.refl >= 1.f || m.roughTex >= 0) return 0.0;
+    float rough = m.rough;
+    if (mattePath) rough = rough * (1. - CAUSTIC_BLUR) + CAUSTIC_BLUR;
+    const float* table = sc.albedo + (size_t)m.table * COS_ENTRIES * ROUGH_ENTRIES;
+    const float c = clampf(dot(lg.Nn, lg.Vn), 0., 1.);
+    const double A = getAlbedo(table, c, rough);
+    int i = std::max(0, std::min(afloor(c * (COS_ENTRIES - 1)), COS_ENTRIES - 1));
+    const int i1 = std::min(i + 1, COS_ENTRIES - 1);
+    const int ra = std::max(0, std::min(afloor(rough * (ROUGH_ENTRIES - 1)), ROUGH_ENTRIES - 1));
+    const int rb = ROUGH_ENTRIES - 1;
+    const double mixc = (double)(c * (COS_ENTRIES - 1) - i);
+    const double colA = (1.0 - mixc) * table[i * ROUGH_ENTRIES + ra] + mixc * table[i1 * ROUGH_ENTRIES + ra];
+    const double colB = (1.0 - mixc) * table[i * ROUGH_ENTRIES + rb] + mixc * table[i1 * ROUGH_ENTRIES + rb];
+    const double dA = (colB - colA) * (ROUGH_ENTRIES - 1) * (mattePath ? 1.0 - CAUSTIC_BLUR : 1.0);
+    if (b.type == SpecBrdf) return (A > 0.0 && A < 1.0) ? dA / A : 0.0;
+    return A < 1.0 ? -dA / (1.0 - A) : 0.0;
+}
+
+struct DThroughput { long base; bool perChannel; double d[3]; };
+
+static void addDT(std::vector<DThroughput>& dT, long base, bool perChannel, const double v[3]) {
+    for (auto& e : dT)
+        if (e.base == base && e.perChannel == perChannel) { for (int c = 0; c < 3; ++c) e.d[c] += v[c]; return; }
+    dT.push_back({base, perChannel, {v[0], v[1], v[2]}});
+}
+
+// One camera path: the forward arithmetic of integrateCameraSample, plus the derivative
+// of <delta, L> added (times the firefly factor) to grad.
+static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, int maxDepth, int minDepth,
+                                const double delta[3], double* grad) {
+    Counts cnt;
+    Ray ray = convertSample(sc, x, y, rng(0), rng(1));
+    int prim; float t, u, v;
+    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) return;
+    Color Lo(0.f);
+    float continueProbability = 1.f;
+    Color pathThroughput(1.f);
+    bool mattePath = false;
+    int rayType = CameraRay;
+    int bounces = 0, trueBounces = 0;
+    std::vector<DThroughput> dT;
+    std::vector<std::pair<long, double>> contrib;
+    while (trueBounces < maxDepth) {
+        LocalGeometry lg = hitGeometry(sc, ray, prim, t, u, v);
+        const int vtx = trueBounces;
+        if (rayType == DiffuseRay) mattePath = true;
+        if (rayType == CameraRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
+        const float lobeU = rng(vdim(vtx, DIM_LOBE));
+        const int matId = sc.attrMat[lg.attr];
+        BrdfState brdf = getBrdf(sc, matId, lg.Vn, lg.Nn, lg.su, lg.sv, mattePath, lobeU);
+        const double T[3] = {pathThroughput.r, pathThroughput.g, pathThroughput.b};
+        const double score = kelemenScore(sc, sc.mats[matId], lg, brdf, mattePath);
+        if (score != 0.0) {
+            const double s3[3] = {T[0] * score, T[1] * score, T[2] * score};
+            addDT(dT, 4L * matId + 3, false, s3);
+        }
+        const ParamRef pr = paramOf(sc, matId, brdf, lg, mattePath, lobeU);
+        DirectGrad dg;
+        Color D = integrateDirect(sc, lg, brdf, rng, vtx, cnt, &dg);
+        Lo += D * pathThroughput;
+        const double Dd[3] = {D.r, D.g, D.b};
+        for (const auto& e : dT) {
+            if (e.perChannel) for (int c = 0; c < 3; ++c) contrib.push_back({e.base + c, delta[c] * e.d[c] * Dd[c]});
+            else contrib.push_back({e.base, delta[0] * e.d[0] * Dd[0] + delta[1] * e.d[1] * Dd[1] + delta[2] * e.d[2] * Dd[2]});
+        }
+        if (pr.base >= 0) {
+            if (pr.perChannel) for (int c = 0; c < 3; ++c) contrib.push_back({pr.base + c, delta[c] * T[c] * dg.dAlbedo[c]});
+            else contrib.push_back({pr.base, pr.chain * (delta[0] * T[0] * dg.dRough[0] + delta[1] * T[1] * dg.dRough[1] +
+                                                          delta[2] * T[2] * dg.dRough[2])});
+        }
+        Sample3D cur = brdfGetSample(brdf, lg.Vn, lg.Nn, rng(vdim(vtx, DIM_BRDF)), rng(vdim(vtx, DIM_BRDF + 1)));
+        if (cur.pdf <= 0.f) break;
+        const float cosl = dot(lg.Nn, cur.ray.direction);
+        const double w[3] = {(double)cur.color.r * cosl / cur.pdf, (double)cur.color.g * cosl / cur.pdf,
+                             (double)cur.color.b * cosl / cur.pdf};
+        double dw[3] = {0, 0, 0};
+        if (pr.base >= 0) {
+            if (pr.perChannel) {
+                for (int c = 0; c < 3; ++c) dw[c] = (double)cosl / cur.pdf / M_PI;   // w_c = albedo_c / pi cos / pdf
+            } else {
+                const double g = dlnBeckmannSampled(brdf, cur.ray.direction, lg.Vn, lg.Nn) * pr.chain;
+                for (int c = 0; c < 3; ++c) dw[c] = w[c] * g;
+            }
+        }
+        for (auto& e : dT) for (int c = 0; c < 3; ++c) e.d[c] *= w[c];
+        if (pr.base >= 0) {
+            const double add[3] = {T[0] * dw[0], T[1] * dw[1], T[2] * dw[2]};
+            addDT(dT, pr.base, pr.perChannel, add);
+        }
+        pathThroughput *= cur.color * dot(lg.Nn, cur.ray.direction) / cur.pdf;
+        if (bounces > minDepth) continueProbability *= cur.color.lum() * dot(lg.Nn, cur.ray.direction) / cur.pdf;
+        if (pathThroughput.isBlack()) break;
+        rayType = brdf.type == SpecBrdf ? SpecularRay : DiffuseRay;
+        if (bounces > minDepth) {
+            if (rng(vdim(vtx, DIM_ROULETTE)) > continueProbability) break;
+            pathThroughput /= continueProbability;
+            for (auto& e : dT) for (int c = 0; c < 3; ++c) e.d[c] /= continueProbability;
+        }
+        cur.ray.origin = lg.P;
+        ++trueBounces;
+        ++bounces;
+        if (trueBounces >= maxDepth) break;
+        ray = cur.ray;
+        if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) break;
+    }
+    if (!std::isfinite(Lo.r) || !std::isfinite(Lo.g) || !std::isfinite(Lo.b)) return;   // dropped, as the forward
+    double clamp = 1.0;
+    while (Lo.r > FIREFLY || Lo.g > FIREFLY || Lo.b > FIREFLY) { Lo *= 0.2f; clamp *= 0.2; }
+    for (const auto& c : contrib) grad[c.first] += clamp * c.second;
 }
 
 // ------------------------------------------------------------ scene import
@@ -821,7 +1023,7 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
     }
     size_t off = 0;
     for (uint32_t t = 0; t < d->ntex; ++t) {
-        Tex tx; tx.w = d->tex_dims[2 * t]; tx.h = d->tex_dims[2 * t + 1]; tx.px = nullptr;
+        Tex tx; tx.w = d->tex_dims[2 * t]; tx.h = d->tex_dims[2 * t + 1]; tx.px = nullptr; tx.offset = off;
         sc->texs.push_back(tx);
         off += 3 * (size_t)tx.w * tx.h;
     }
@@ -970,6 +1172,38 @@ int oracle_render(void* h, int spp, int sample_offset, int max_depth, int min_de
         cl += cnt.closest; sh += cnt.shadow;
     }
     if (counts) { counts[0] += cl; counts[1] += sh; counts[2] += (uint64_t)w * hgt * spp; }
+    return 0;
+}
+
+// dLoss/dparams of <dfilm, image> restricted to pixels [x0, x0+w) x [y0, y0+h), with
+// dfilm the full W*H*4 image gradient (alpha ignored) and the image the spp-sample mean.
+// grad: 4*nmat + ntexel_floats doubles (overwritten).
+int oracle_adjoint(void* h, int spp, int sample_offset, int max_depth, int min_depth, uint32_t seed, int threads,
+                   int x0, int y0, int w, int hgt, const float* dfilm, double* grad) {
+    const Scene& sc = *(Scene*)h;
+    const size_t np = 4 * sc.mats.size() + sc.texels.size();
+    if (threads > 0) omp_set_num_threads(threads);
+    const uint64_t key = key_of(seed);
+    std::fill(grad, grad + np, 0.0);
+#pragma omp parallel
+    {
+        std::vector<double> local(np, 0.0);
+#pragma omp for schedule(dynamic, 4)
+        for (long long i = 0; i < (long long)w * hgt; ++i) {
+            const int x = x0 + (int)(i % w), y = y0 + (int)(i / w);
+            const uint32_t pixel = (uint32_t)y * (uint32_t)sc.width + (uint32_t)x;
+            const double delta[3] = {(double)dfilm[4 * (size_t)pixel] / spp, (double)dfilm[4 * (size_t)pixel + 1] / spp,
+                                     (double)dfilm[4 * (size_t)pixel + 2] / spp};
+            if (delta[0] == 0 && delta[1] == 0 && delta[2] == 0) continue;
+            for (int s = 0; s < spp; ++s) {
+                Rng rng; rng.key = key;
+                rng.base = ((uint64_t)pixel << 32) | ((uint64_t)(sample_offset + s) << 12);
+                adjointCameraSample(sc, x, y, rng, max_depth, min_depth, delta, local.data());
+            }
+        }
+#pragma omp critical
+        for (size_t k = 0; k < np; ++k) grad[k] += local[k];
+    }
     return 0;
 }
 

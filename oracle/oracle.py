@@ -40,6 +40,7 @@ def lib() -> C.CDLL:
         L.oracle_render.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp, vp]
         L.oracle_kelemen_table.argtypes = [C.c_float, i32, u32, vp, i32]
         L.oracle_shading_probe.argtypes = [vp, i32, vp, u32, vp, vp]
+        L.oracle_adjoint.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp]
         _lib = L
     return _lib
 
@@ -112,6 +113,19 @@ class OracleScene:
         lib().oracle_render(self.h, spp, sample_offset, max_depth, min_depth, seed, threads, x0, y0, w, h,
                             mean.ctypes.data, None if m2 is None else m2.ctypes.data, counts.ctypes.data)
         return mean, m2, counts
+
+    def adjoint(self, spp, max_depth, min_depth, seed, dfilm, crop=None, sample_offset=0, threads=0):
+        """FP64 gradient of <dfilm, image> w.r.t. (per material: diffuse rgb, roughness) and the
+        texels, over the crop's pixels. Returns (grad_mat [nmat, 4], grad_tex [ntexel floats])."""
+        W, H = self.data.width, self.data.height
+        x0, y0, w, h = crop if crop is not None else (0, 0, W, H)
+        dfilm = np.ascontiguousarray(dfilm, np.float32).reshape(H * W * 4)
+        nmat = len(self.data.materials)
+        ntex = int(self.data.texels().size)
+        grad = np.zeros(4 * nmat + ntex, np.float64)
+        lib().oracle_adjoint(self.h, spp, sample_offset, max_depth, min_depth, seed, threads, x0, y0, w, h,
+                             dfilm.ctypes.data, grad.ctypes.data)
+        return grad[:4 * nmat].reshape(nmat, 4), grad[4 * nmat:]
 
     def probe(self, kind, records):
         records = np.ascontiguousarray(records, np.float32)

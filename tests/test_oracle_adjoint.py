@@ -1,0 +1,76 @@
+"""Pins the oracle's FP64 adjoint (oracle_adjoint, forward-mode) against central finite
+differences of the oracle's own renderer.
+
+With roulette off, a diffuse colour or a texel enters each path sample polynomially
+(Lambert sampling does not depend on it), so with common random numbers the central
+difference of the rendered loss equals the adjoint sample by sample up to O(h^2) and
+float rounding. Tolerance: 1% of the finite difference plus 1e-6 absolute.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+
+def _loss(oracle_lib, data, tables, w, spp, crop, seed):
+    osc = oracle_lib.OracleScene(data, tables, use_bvh=True)
+    mean, _, _ = osc.render(spp, data.render["max_depth"], data.render["min_depth"], seed, crop=crop, want_m2=False)
+    x0, y0, cw, ch = crop
+    return float(np.sum(mean[..., :3] * w[y0:y0 + ch, x0:x0 + cw, :3]))
+
+
+def _perturbed_material(data, m, c, h):
+    d = copy.copy(data)
+    d.materials = list(data.materials)
+    md = copy.copy(data.materials[m])
+    md.diffuse[c] = md.diffuse[c] + h
+    d.materials[m] = md
+    return d
+
+
+def _perturbed_texel(data, i, h):
+    d = copy.copy(data)
+    tex = [np.array(t, np.float32, copy=True) for t in data.textures]
+    flat = tex[0].reshape(-1)
+    flat[i] = flat[i] + h
+    d.textures = tex
+    return d
+
+
+def test_oracle_adjoint_albedo_matches_fd(oracle_lib):
+    from aurora_b200 import scenes
+    data = scenes.box_scene(64, 64, spp=8)
+    tables = np.zeros((21, 64, 32), np.float32)
+    w = np.random.default_rng(5).normal(size=(64, 64, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    crop, spp, seed = (16, 16, 32, 32), 8, 1
+    osc = oracle_lib.OracleScene(data, tables, use_bvh=True)
+    gm, gt = osc.adjoint(spp, 5, 5, seed, w, crop=crop)
+    assert gt.size == 0
+    h = 1e-2
+    for m, c in [(0, 0), (0, 2), (1, 0), (2, 1)]:     # walls, red wall, green wall
+        fd = (_loss(oracle_lib, _perturbed_material(data, m, c, h), tables, w, spp, crop, seed) -
+              _loss(oracle_lib, _perturbed_material(data, m, c, -h), tables, w, spp, crop, seed)) / (2 * h)
+        assert abs(gm[m, c] - fd) <= 0.01 * abs(fd) + 1e-6, (m, c, gm[m, c], fd)
+    # the Cook-Torrance boxes' albedo is not a parameter; the lights' constant material neither
+    assert np.all(gm[4:, :3] == 0.0)
+
+
+def test_oracle_adjoint_texel_matches_fd(oracle_lib):
+    from aurora_b200 import scenes
+    data = scenes.texture_scene(128, 128, spp=4)
+    tables = np.zeros((21, 64, 32), np.float32)
+    tables[10] = oracle_lib.kelemen_table(0.5, 400)          # the sphere's Kelemen material (reflectance 0.5)
+    w = np.random.default_rng(6).normal(size=(128, 128, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    crop, spp, seed = (48, 88, 32, 32), 4, 2                  # ground in front of the sphere
+    osc = oracle_lib.OracleScene(data, tables, use_bvh=True)
+    gm, gt = osc.adjoint(spp, 6, 6, seed, w, crop=crop)
+    assert gt.size == data.texels().size and np.count_nonzero(gt) > 0
+    i = int(np.argmax(np.abs(gt)))
+    h = 1e-2
+    fd = (_loss(oracle_lib, _perturbed_texel(data, i, h), tables, w, spp, crop, seed) -
+          _loss(oracle_lib, _perturbed_texel(data, i, -h), tables, w, spp, crop, seed)) / (2 * h)
+    assert abs(gt[i] - fd) <= 0.01 * abs(fd) + 1e-6, (i, gt[i], fd)
+    # the textured ground owns no constant diffuse gradient
+    assert np.all(gm[0, :3] == 0.0)
