@@ -31,7 +31,10 @@ constexpr int kAdjBlock = 128;
 constexpr int kAdjMaxDepth = 16;
 constexpr int kAdjMaxMat = 64;
 
-struct VtxRec { int prim; float t, u, v; uint32_t vis; };
+// hit record of one vertex: (t, u, v, prim | visibility of its next-event rays << 30)
+__device__ __forceinline__ float4 pack_rec(const Hit& h, uint32_t vis) {
+    return make_float4(h.t, h.u, h.v, __int_as_float(h.prim | (int)(vis << 30)));
+}
 
 // atomic add with the exact rounding error of that addition sent to a compensation slot
 __device__ __forceinline__ void comp_add(float* sum, float* comp, float x) {
@@ -205,6 +208,107 @@ __device__ __forceinline__ ParamRef param_of(const ShadeScene& sh, int mat_id, c
     return p;
 }
 
+// Pass 2 of one camera path: re-shades the recorded vertices rec[0, nv) (no ray
+// tracing) and accumulates dL/dtheta with delta = dLoss/dpixel / spp. Lo is the path's
+// unclamped radiance from pass 1.
+__device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams& p, int px, int py,
+                                            const PathRng& rng, const float4* rec, int nv, float3 Lo, float3 delta,
+                                            float* s_g, float* s_c, float* g_tex, float* g_tex_c, RayCounts& rc) {
+    if (nv == 0 || !isfinite(Lo.x) || !isfinite(Lo.y) || !isfinite(Lo.z)) return;
+    float clampf = 1.f;             // firefly clamp factor (detached)
+    {
+        float3 c = Lo;
+        for (int k = 0; k < 64 && (c.x > kFirefly || c.y > kFirefly || c.z > kFirefly); ++k) { c *= 0.2f; clampf *= 0.2f; }
+    }
+    const float3 dp = delta * clampf;
+    RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+    float3 T = mk(1.f, 1.f, 1.f), collected = mk(0.f, 0.f, 0.f);
+    float cont = 1.f;
+    bool matte = false;
+    int kind = RAY_CAMERA, bounces = 0;
+    for (int vtx = 0; vtx < nv; ++vtx) {
+        const float4 r = rec[vtx];
+        const uint32_t bits = __float_as_uint(r.w);
+        const int prim = (int)(bits & 0x3fffffffu);
+        uint32_t vis = bits >> 30;
+        const Frame f = hit_frame(sc.sh, prim, r.x, r.y, r.z, ray.o, ray.d, true);
+        const Attr at = sc.sh.attrs[f.attr];
+        if (kind == RAY_DIFFUSE) matte = true;
+        if (kind == RAY_CAMERA) collected += T * at.emission;
+        const float lobe_u = rng.u(vertex_dim(vtx, kDimLobe));
+        const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte, lobe_u);
+        const ParamRef pr = param_of(sc.sh, at.material, brdf, f, matte, lobe_u);
+        float3 dD;
+        const float3 D = direct<false, true>(sc, f, brdf, rng, vtx, rc, &vis, &dD);
+        collected += D * T;
+        const float3 gdir = T * dD;
+        const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
+                                          rng.u(vertex_dim(vtx, kDimBrdf + 1)));
+        float3 gcont = mk(0.f, 0.f, 0.f);
+        float3 w = mk(0.f, 0.f, 0.f);
+        const bool cont_ok = bs.pdf > 0.f;
+        const float3 after = Lo - collected;
+        const Material mat = sc.sh.mats[at.material];
+        if (mat.type == MAT_KELEMEN && mat.refl < 1.f && mat.rough_tex < 0) {
+            // the lobe choice depends on roughness: score-function term on the subtree radiance
+            const float score = kelemen_score(sc.sh, mat, f, brdf, matte);
+            const float3 sub = dp * (D * T + after);
+            comp_add(&s_g[4 * at.material + 3], &s_c[4 * at.material + 3], score * (sub.x + sub.y + sub.z));
+        }
+        if (cont_ok && pr.kind != 0) {
+            const float cosl = dot(f.N, bs.dir);
+            w = cdiv(bs.color * cosl, bs.pdf);
+            if (pr.kind == 3) {
+                const float g = sample_dlnD(brdf, f, bs);   // dw/w = d ln f
+                gcont = after * g;
+            } else {
+                const float dw = kInvPiMacro * cosl / bs.pdf;  // d w_c / d diffuse_c
+                gcont = mk(w.x != 0.f ? after.x * dw / w.x : 0.f, w.y != 0.f ? after.y * dw / w.y : 0.f,
+                           w.z != 0.f ? after.z * dw / w.z : 0.f);
+            }
+        }
+        if (pr.kind == 1 || pr.kind == 2) {
+            const float3 g = dp * (gdir + gcont);
+            if (pr.kind == 1) {
+                comp_add(&s_g[4 * pr.index + 0], &s_c[4 * pr.index + 0], g.x);
+                comp_add(&s_g[4 * pr.index + 1], &s_c[4 * pr.index + 1], g.y);
+                comp_add(&s_g[4 * pr.index + 2], &s_c[4 * pr.index + 2], g.z);
+            } else {
+                comp_add(&g_tex[3 * pr.index + 0], &g_tex_c[3 * pr.index + 0], g.x);
+                comp_add(&g_tex[3 * pr.index + 1], &g_tex_c[3 * pr.index + 1], g.y);
+                comp_add(&g_tex[3 * pr.index + 2], &g_tex_c[3 * pr.index + 2], g.z);
+            }
+        } else if (pr.kind == 3) {
+            const float3 g = dp * (gdir * pr.dr + gcont * pr.dr);
+            comp_add(&s_g[4 * pr.index + 3], &s_c[4 * pr.index + 3], g.x + g.y + g.z);
+        }
+        // the forward update, identical to pass 1
+        if (!cont_ok) break;
+        const float cosl = dot(f.N, bs.dir);
+        T *= cdiv(bs.color * cosl, bs.pdf);
+        if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
+        if (is_black(T)) break;
+        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
+        if (bounces > p.min_depth) {
+            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
+            T = cdiv(T, cont);
+        }
+        ++bounces;
+        ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
+    }
+}
+
+// the block's material gradients (sum and compensation) go to the global ones
+__device__ __forceinline__ void flush_block(const float* s_g, const float* s_c, int nmat, float* g_mat, float* g_mat_c) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < nmat * 4; i += blockDim.x) {
+        comp_add(&g_mat[i], &g_mat_c[i], s_g[i]);
+        comp_add(&g_mat[i], &g_mat_c[i], s_c[i]);
+    }
+}
+
+// Megakernel form: one thread per pixel runs pass 1 (forward with tracing, records in
+// thread-local memory) and pass 2 for each of its samples.
 __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p, const float4* __restrict__ dfilm,
                                                        int nmat, float* g_mat, float* g_mat_c, float* g_tex,
                                                        float* g_tex_c, unsigned long long* counters) {
@@ -224,8 +328,8 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
         const bool any = delta.x != 0.f || delta.y != 0.f || delta.z != 0.f;
         for (int s = 0; any && s < p.spp; ++s) {
             rng.base = path_base((uint32_t)pixel, (uint32_t)(p.sample_offset + s));
-            // ---------------- pass 1: forward replay, recording hits and visibility
-            VtxRec rec[kAdjMaxDepth];
+            // ---------------- pass 1: forward, recording hits and visibility
+            float4 rec[kAdjMaxDepth];
             int nv = 0;
             float3 Lo = mk(0.f, 0.f, 0.f);
             {
@@ -238,7 +342,6 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                     bool matte = false;
                     int kind = RAY_CAMERA, bounces = 0;
                     for (int vtx = 0; vtx < p.max_depth; ++vtx) {
-                        rec[vtx] = {h.prim, h.t, h.u, h.v, 0u};
                         nv = vtx + 1;
                         const Frame f = hit_frame(sc.sh, h.prim, h.t, h.u, h.v, ray.o, ray.d, true);
                         const Attr at = sc.sh.attrs[f.attr];
@@ -246,7 +349,9 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         if (kind == RAY_CAMERA) Lo += T * at.emission;
                         const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
                                                    rng.u(vertex_dim(vtx, kDimLobe)));
-                        Lo += direct<true, false>(sc, f, brdf, rng, vtx, rc, &rec[vtx].vis, nullptr) * T;
+                        uint32_t vis = 0;
+                        Lo += direct<true, false>(sc, f, brdf, rng, vtx, rc, &vis, nullptr) * T;
+                        rec[vtx] = pack_rec(h, vis);
                         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
                         if (bs.pdf <= 0.f) break;
@@ -267,94 +372,11 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                     }
                 }
             }
-            if (nv == 0 || !isfinite(Lo.x) || !isfinite(Lo.y) || !isfinite(Lo.z)) continue;
-            float clampf = 1.f;             // firefly clamp factor (detached)
-            {
-                float3 c = Lo;
-                for (int k = 0; k < 64 && (c.x > kFirefly || c.y > kFirefly || c.z > kFirefly); ++k) { c *= 0.2f; clampf *= 0.2f; }
-            }
-            const float3 dp = delta * clampf;
             // ---------------- pass 2: re-shade the recorded vertices, accumulate gradients
-            RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
-            float3 T = mk(1.f, 1.f, 1.f), collected = mk(0.f, 0.f, 0.f);
-            float cont = 1.f;
-            bool matte = false;
-            int kind = RAY_CAMERA, bounces = 0;
-            for (int vtx = 0; vtx < nv; ++vtx) {
-                const VtxRec r = rec[vtx];
-                const Frame f = hit_frame(sc.sh, r.prim, r.t, r.u, r.v, ray.o, ray.d, true);
-                const Attr at = sc.sh.attrs[f.attr];
-                if (kind == RAY_DIFFUSE) matte = true;
-                if (kind == RAY_CAMERA) collected += T * at.emission;
-                const float lobe_u = rng.u(vertex_dim(vtx, kDimLobe));
-                const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte, lobe_u);
-                const ParamRef pr = param_of(sc.sh, at.material, brdf, f, matte, lobe_u);
-                uint32_t vis = r.vis;
-                float3 dD;
-                const float3 D = direct<false, true>(sc, f, brdf, rng, vtx, rc, &vis, &dD);
-                collected += D * T;
-                const float3 gdir = T * dD;
-                const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
-                                                  rng.u(vertex_dim(vtx, kDimBrdf + 1)));
-                float3 gcont = mk(0.f, 0.f, 0.f);
-                float3 w = mk(0.f, 0.f, 0.f);
-                const bool cont_ok = bs.pdf > 0.f;
-                const float3 after = Lo - collected;
-                const Material mat = sc.sh.mats[at.material];
-                if (mat.type == MAT_KELEMEN && mat.refl < 1.f && mat.rough_tex < 0) {
-                    // the lobe choice depends on roughness: score-function term on the subtree radiance
-                    const float score = kelemen_score(sc.sh, mat, f, brdf, matte);
-                    const float3 sub = dp * (D * T + after);
-                    comp_add(&s_g[4 * at.material + 3], &s_c[4 * at.material + 3], score * (sub.x + sub.y + sub.z));
-                }
-                if (cont_ok && pr.kind != 0) {
-                    const float cosl = dot(f.N, bs.dir);
-                    w = cdiv(bs.color * cosl, bs.pdf);
-                    if (pr.kind == 3) {
-                        const float g = sample_dlnD(brdf, f, bs);   // dw/w = d ln f
-                        gcont = after * g;
-                    } else {
-                        const float dw = kInvPiMacro * cosl / bs.pdf;  // d w_c / d diffuse_c
-                        gcont = mk(w.x != 0.f ? after.x * dw / w.x : 0.f, w.y != 0.f ? after.y * dw / w.y : 0.f,
-                                   w.z != 0.f ? after.z * dw / w.z : 0.f);
-                    }
-                }
-                if (pr.kind == 1 || pr.kind == 2) {
-                    const float3 g = dp * (gdir + gcont);
-                    if (pr.kind == 1) {
-                        comp_add(&s_g[4 * pr.index + 0], &s_c[4 * pr.index + 0], g.x);
-                        comp_add(&s_g[4 * pr.index + 1], &s_c[4 * pr.index + 1], g.y);
-                        comp_add(&s_g[4 * pr.index + 2], &s_c[4 * pr.index + 2], g.z);
-                    } else {
-                        comp_add(&g_tex[3 * pr.index + 0], &g_tex_c[3 * pr.index + 0], g.x);
-                        comp_add(&g_tex[3 * pr.index + 1], &g_tex_c[3 * pr.index + 1], g.y);
-                        comp_add(&g_tex[3 * pr.index + 2], &g_tex_c[3 * pr.index + 2], g.z);
-                    }
-                } else if (pr.kind == 3) {
-                    const float3 g = dp * (gdir * pr.dr + gcont * pr.dr);
-                    comp_add(&s_g[4 * pr.index + 3], &s_c[4 * pr.index + 3], g.x + g.y + g.z);
-                }
-                // the forward update, identical to pass 1
-                if (!cont_ok) break;
-                const float cosl = dot(f.N, bs.dir);
-                T *= cdiv(bs.color * cosl, bs.pdf);
-                if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
-                if (is_black(T)) break;
-                kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
-                if (bounces > p.min_depth) {
-                    if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
-                    T = cdiv(T, cont);
-                }
-                ++bounces;
-                ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
-            }
+            replay_path(sc, p, px, py, rng, rec, nv, Lo, delta, s_g, s_c, g_tex, g_tex_c, rc);
         }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < nmat * 4; i += blockDim.x) {
-        comp_add(&g_mat[i], &g_mat_c[i], s_g[i]);
-        comp_add(&g_mat[i], &g_mat_c[i], s_c[i]);
-    }
+    flush_block(s_g, s_c, nmat, g_mat, g_mat_c);
     unsigned long long v[3] = {rc.closest, rc.shadow, pixel < npix ? (unsigned long long)p.spp : 0ull};
 #pragma unroll
     for (int k = 0; k < 3; ++k)
@@ -362,6 +384,38 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
         for (int o = 16; o > 0; o >>= 1) v[k] += __shfl_xor_sync(0xffffffffu, v[k], o);
     if ((threadIdx.x & 31) == 0)
         for (int k = 0; k < 3; ++k) atomicAdd(&counters[k], v[k]);
+}
+
+// Replay form (pass 2 only): one thread per item of a record pass (sample-major:
+// sl * npix + pixel, sample index p.sample_offset + s0 + sl). The wavefront engine's
+// record pass wrote the hit records rec[item][p.max_depth] and lo_raw[item].
+__global__ void __launch_bounds__(kAdjBlock) k_adjoint_replay(DevScene sc, PathParams p, int s0, uint32_t items,
+                                                              const float4* __restrict__ rec,
+                                                              const float4* __restrict__ lo_raw,
+                                                              const float4* __restrict__ dfilm, int nmat, float* g_mat,
+                                                              float* g_mat_c, float* g_tex, float* g_tex_c) {
+    __shared__ float s_g[kAdjMaxMat * 4], s_c[kAdjMaxMat * 4];
+    for (int i = threadIdx.x; i < nmat * 4; i += blockDim.x) { s_g[i] = 0.f; s_c[i] = 0.f; }
+    __syncthreads();
+    const uint32_t npix = (uint32_t)(sc.cam.w * sc.cam.h);
+    const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
+    RayCounts rc;
+    if (item < items) {
+        const uint32_t pixel = item % npix, sl = item / npix;
+        const float4 df = dfilm[pixel];
+        const float inv = 1.f / (float)p.spp;
+        const float3 delta = mk(df.x * inv, df.y * inv, df.z * inv);
+        if (delta.x != 0.f || delta.y != 0.f || delta.z != 0.f) {
+            PathRng rng;
+            rng.key = seed_key(p.seed);
+            rng.base = path_base(pixel, (uint32_t)(p.sample_offset + s0) + sl);
+            const float4 lo = lo_raw[item];
+            replay_path(sc, p, (int)(pixel % (uint32_t)sc.cam.w), (int)(pixel / (uint32_t)sc.cam.w), rng,
+                        rec + (size_t)item * p.max_depth, __float_as_int(lo.w), mk(lo.x, lo.y, lo.z), delta, s_g, s_c,
+                        g_tex, g_tex_c, rc);
+        }
+    }
+    flush_block(s_g, s_c, nmat, g_mat, g_mat_c);
 }
 
 __global__ void k_add_comp(float* g, const float* c, int n) {
@@ -382,6 +436,10 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
     aur_status st = render_options(sc, o, &p);
     if (st != AUR_OK) return st;
     if (o->max_depth > kAdjMaxDepth) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: max_depth above 16");
+    if (o->mode != AUR_RENDER_PLAIN && o->mode != AUR_RENDER_WAVEFRONT)
+        return fail(AUR_ERR_INVALID_ARG, "aur_render_adjoint: unknown mode");
+    const bool wavefront = o->mode == AUR_RENDER_WAVEFRONT;
+    if (sc->ntri >= (1u << 30)) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: 2^30 triangles or more");
     const int nmat = (int)sc->h_mats.size();
     if (nmat > kAdjMaxMat) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: more than 64 materials");
     DeviceGuard g(sc->ctx->device);
@@ -404,28 +462,62 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     cudaEventRecord(e0, s);
-    if (e == cudaSuccess) {
+    uint64_t launches = 0;
+    unsigned long long rays[2] = {0, 0};
+    float4* rec = nullptr;
+    if (wavefront) {
+        // record passes (wavefront engine) + replay kernels over chunks of the samples, sized
+        // so that the records stay within 2 GiB and item indices within 2^31
+        const size_t per_item = sizeof(float4) * ((size_t)p.max_depth + 1);
+        const size_t budget = (size_t)2 << 30;
+        int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)p.spp, budget / (per_item * npix)));
+        while (chunk > 1 && (size_t)chunk * npix * (p.max_depth + 1) >= (1ull << 31)) chunk /= 2;
+        if ((size_t)chunk * npix * (p.max_depth + 1) >= (1ull << 31)) e = cudaErrorInvalidValue;
+        if (e == cudaSuccess) e = cudaMallocAsync(&rec, per_item * npix * chunk, s);
+        float4* lo_raw = rec ? rec + (size_t)npix * chunk * p.max_depth : nullptr;
+        for (int s0 = 0; s0 < p.spp && e == cudaSuccess; s0 += chunk) {
+            const int n = std::min(chunk, p.spp - s0);
+            aur_status rs = wf_record_pass(sc, p, s0, n, rec, lo_raw, &launches, rays);
+            if (rs != AUR_OK) {
+                if (cm) cudaFreeAsync(cm, s);
+                if (rec) cudaFreeAsync(rec, s);
+                cudaEventDestroy(e0);
+                cudaEventDestroy(e1);
+                return rs;
+            }
+            const uint32_t items = (uint32_t)(npix * (size_t)n);
+            k_adjoint_replay<<<(items + kAdjBlock - 1) / kAdjBlock, kAdjBlock, 0, s>>>(
+                sc->dev(), p, s0, items, rec, lo_raw, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
+                ntex ? (float*)gt.ptr : nullptr, ct);
+            ++launches;
+            e = cudaGetLastError();
+        }
+    } else if (e == cudaSuccess) {
         k_adjoint<<<(unsigned)((npix + kAdjBlock - 1) / kAdjBlock), kAdjBlock, 0, s>>>(
             sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm, ntex ? (float*)gt.ptr : nullptr, ct,
             sc->ctx->counters);
+        ++launches;
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {
         k_add_comp<<<(4 * nmat + 255) / 256, 256, 0, s>>>((float*)gm.ptr, cm, 4 * nmat);
-        if (ntex) k_add_comp<<<(ntex + 255) / 256, 256, 0, s>>>((float*)gt.ptr, ct, ntex);
+        ++launches;
+        if (ntex) { k_add_comp<<<(ntex + 255) / 256, 256, 0, s>>>((float*)gt.ptr, ct, ntex); ++launches; }
         e = cudaGetLastError();
     }
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) e = gm.finish();
     if (e == cudaSuccess && ntex) e = gt.finish();
-    unsigned long long cnt[3] = {0, 0, 0};
-    if (e == cudaSuccess) e = cudaMemcpyAsync(cnt, sc->ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
+    unsigned long long cnt[3] = {rays[0], rays[1], (unsigned long long)npix * p.spp};
+    if (e == cudaSuccess && !wavefront)
+        e = cudaMemcpyAsync(cnt, sc->ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     float ms = 0.f;
     if (e == cudaSuccess) cudaEventElapsedTime(&ms, e0, e1);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (cm) cudaFreeAsync(cm, s);
+    if (rec) cudaFreeAsync(rec, s);
     if (e != cudaSuccess) return cuda_fail(e, "aur_render_adjoint");
     if (stats) {
         *stats = aur_render_stats{};
@@ -433,7 +525,7 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
         stats->shadow_rays = cnt[1];
         stats->paths = cnt[2];
         stats->camera_rays = cnt[2];
-        stats->launches = ntex ? 3 : 2;
+        stats->launches = launches;
         stats->kernel_ms = ms;
     }
     return AUR_OK;

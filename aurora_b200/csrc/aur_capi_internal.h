@@ -62,6 +62,8 @@ aur_status bvh_options(const aur_bvh_opts* o, BvhBuildOptions* out);
 aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathParams* p);
 aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film, aur_render_stats* stats);
 void wf_release_context(aur_ctx* ctx);   // frees the wavefront engines cached for a context
+aur_status wf_record_pass(aur_scene* sc, const PathParams& p, int s0, int nsamples, float4* rec, float4* lo_raw,
+                          uint64_t* launches, unsigned long long* rays);
 
 struct DeviceGuard {
     explicit DeviceGuard(int dev);

@@ -50,8 +50,11 @@ struct WfScene {
     DevScene sc;
     PathParams p;          // spp = samples of this pass, sample_offset = first sample index of this pass
     uint64_t key;
-    uint32_t npix, item_base, items, pad;
+    uint32_t npix, item_base, items, rec_depth;
     float4* samples;       // [spp_pass][npix]
+    // record mode (path-replay adjoint): per item (sample-major, sl * npix + pixel)
+    float4* rec;           // [items][rec_depth] hit records (t, u, v, prim | visibility << 30)
+    float4* lo_raw;        // [items] unclamped path radiance, w = number of recorded vertices
 };
 
 struct WfPool {
@@ -59,6 +62,7 @@ struct WfPool {
     uint4* id;
     uint32_t* state;            // PS_* in the low bits, PS_PENDING when next-event rays are in flight
     uint32_t* sh_vis;           // bit k: next-event ray k of the slot is unoccluded
+    uint32_t* rec_cur;          // record mode: record index of the vertex whose next-event rays are in flight
     uint32_t *q_ext0, *q_ext1, *q_sort, *q_shadow;
     uint32_t* ctr;
     unsigned long long* rays;   // [0] closest-hit rays, [1] shadow rays
@@ -107,6 +111,7 @@ __device__ __forceinline__ int scene_of(const WfPool& w, uint32_t item) {
 }
 
 // ------------------------------------------------------------------ regen
+template <bool kRec>
 __global__ void k_regen(WfPool w, int in_q) {
     uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
     uint32_t* cin = &w.ctr[in_q ? C_EXT1 : C_EXT0];
@@ -130,13 +135,21 @@ __global__ void k_regen(WfPool w, int in_q) {
             lo.x += add.x; lo.y += add.y; lo.z += add.z;
             w.lo[i] = lo;
             st &= ~PS_PENDING;
+            if (kRec) {   // the visibility of the vertex's next-event rays goes into its record
+                float4* r = w.scenes[w.id[i].x].rec + w.rec_cur[i];
+                r->w = __int_as_float(__float_as_int(r->w) | (int)(vis << 30));
+            }
         }
         if (st == PS_DONE) {
             const uint4 id = w.id[i];
             const WfScene& S = w.scenes[id.x];
             const float4 lo = w.lo[i];
-            const float3 L = firefly_clamp(mk(lo.x, lo.y, lo.z));
-            S.samples[(size_t)id.z * S.npix + id.y] = make_float4(L.x, L.y, L.z, lo.w);
+            if (kRec) {
+                S.lo_raw[(size_t)id.z * S.npix + id.y] = make_float4(lo.x, lo.y, lo.z, __int_as_float(f_vtx(id.w)));
+            } else {
+                const float3 L = firefly_clamp(mk(lo.x, lo.y, lo.z));
+                S.samples[(size_t)id.z * S.npix + id.y] = make_float4(L.x, L.y, L.z, lo.w);
+            }
             st = PS_EMPTY;
         }
         const bool want = st == PS_EMPTY && *(volatile uint32_t*)&w.ctr[C_WORK] < total;
@@ -288,6 +301,7 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
 }
 
 // ------------------------------------------------------------------ shade
+template <bool kRec>
 __global__ void k_shade(WfPool w, int in_q, int sorted) {
     const uint32_t* qin = sorted ? w.q_sort : (in_q ? w.q_ext1 : w.q_ext0);
     const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
@@ -328,6 +342,8 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 float cont = tpv.w;
                 float3 Lo = mk(lo.x, lo.y, lo.z);
                 if (vtx == 0) lo.w = 1.f;   // camera ray hit: alpha
+                const uint32_t rec_at = (id.z * S.npix + id.y) * S.rec_depth + (uint32_t)vtx;
+                if (kRec) S.rec[rec_at] = make_float4(hh.x, hh.y, hh.z, __int_as_float(prim));
                 const Frame f = hit_frame(sc.sh, prim, hh.x, hh.y, hh.z, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), true);
                 const Attr at = sc.sh.attrs[f.attr];
                 if (kind == RAY_DIFFUSE) matte = true;
@@ -377,6 +393,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                             }
                         }
                         if (r0 || r1) {
+                            if (kRec) w.rec_cur[slot] = rec_at;
                             w.sh_p[slot] = make_float4(f.P.x, f.P.y, f.P.z, (float)nvis);
                             w.sh_d0[slot] = make_float4(d0.x, d0.y, d0.z, m0);
                             w.sh_d1[slot] = make_float4(d1.x, d1.y, d1.z, m1);
@@ -417,6 +434,8 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                     }
                 }
                 lo = make_float4(Lo.x, Lo.y, Lo.z, lo.w);
+                // a finished path's flags count its recorded vertices (a missed ray's vertex is not recorded)
+                if (kRec && !alive) w.id[slot].w = pack_flags(vtx + 1, bounces, kind, matte);
                 w.state[slot] = (alive ? PS_ACTIVE : PS_DONE) | (push_sh0 || push_sh1 ? PS_PENDING : 0u);
                 push_ext = alive;
             }
@@ -517,6 +536,7 @@ struct WfConfig {
     uint32_t pool = 1u << 21;
     int block = 128;
     int sort = 1;
+    int record = 0;   // record mode: hit records + unclamped radiance per item instead of samples
 };
 
 // ------------------------------------------------------------------ host driver
@@ -546,7 +566,7 @@ struct WfRun {
         cfg = c;
         stream = s;
         const size_t P = c.pool;
-        const size_t bytes = P * (11 * sizeof(float4) + sizeof(uint4) + 7 * sizeof(uint32_t)) + 19 * 256 +
+        const size_t bytes = P * (11 * sizeof(float4) + sizeof(uint4) + 8 * sizeof(uint32_t)) + 20 * 256 +
                              kCounters * sizeof(uint32_t) + 2 * sizeof(unsigned long long);
         cudaError_t e = cudaMalloc(&mem, bytes);
         if (e != cudaSuccess) return e;
@@ -561,6 +581,7 @@ struct WfRun {
         w.q_sort = (uint32_t*)take(P * 4);
         w.q_shadow = (uint32_t*)take(2 * P * 4);   // up to two next-event rays per slot
         w.sh_vis = (uint32_t*)take(P * 4);
+        w.rec_cur = (uint32_t*)take(P * 4);
         w.ctr = (uint32_t*)take(kCounters * 4);
         w.rays = (unsigned long long*)take(2 * sizeof(unsigned long long));
         if ((size_t)(p - (char*)mem) > bytes) return cudaErrorMemoryAllocation;
@@ -583,7 +604,7 @@ struct WfRun {
             return std::max(1, nb) * sms;
         };
         grid_ext = persist(c.sort ? (const void*)k_extend<true> : (const void*)k_extend<false>, stack_smem);
-        grid_shade = persist((const void*)k_shade, 0);
+        grid_shade = persist(c.record ? (const void*)k_shade<true> : (const void*)k_shade<false>, 0);
         grid_shadow = persist((const void*)k_shadow, stack_smem);
         grid_sort = persist((const void*)k_sort_scatter, 0);
         grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 16);
@@ -594,14 +615,16 @@ struct WfRun {
     void enqueue_iteration(int in_q, int it) {
         // inside stream capture only an "external" record becomes an event-record node
         cudaEvent_t* e = &ev[it * kStages + 1];
-        k_regen<<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
+        if (cfg.record) k_regen<true><<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
+        else k_regen<false><<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[0], stream, cudaEventRecordExternal);
         if (cfg.sort) k_extend<true><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
         else k_extend<false><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[1], stream, cudaEventRecordExternal);
         if (cfg.sort) k_sort_scatter<<<grid_sort, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[2], stream, cudaEventRecordExternal);
-        k_shade<<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
+        if (cfg.record) k_shade<true><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
+        else k_shade<false><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
         cudaEventRecordWithFlags(e[3], stream, cudaEventRecordExternal);
         k_shadow<<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
         cudaEventRecordWithFlags(e[4], stream, cudaEventRecordExternal);
@@ -644,7 +667,9 @@ struct WfRun {
                 else cudaGetLastError();   // timing is informational; never leave a stale error behind
             }
             if (h_ctr[C_WORK] >= total && h_ctr[C_EXT0] == 0) {
-                k_regen<<<grid_regen, cfg.block, 0, stream>>>(w, 0);   // writes the last finished samples
+                // writes the last finished samples
+                if (cfg.record) k_regen<true><<<grid_regen, cfg.block, 0, stream>>>(w, 0);
+                else k_regen<false><<<grid_regen, cfg.block, 0, stream>>>(w, 0);
                 *launches += 1;
                 return cudaGetLastError();
             }
@@ -787,11 +812,11 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
 // Engines (pool buffers, captured graph, events, sample buffer) are cached per
 // (context, configuration) and reused by later calls; aur_ctx_destroy releases them.
 static std::mutex g_engine_mutex;
-static std::map<std::tuple<aur_ctx*, uint32_t, int, int>, std::unique_ptr<WfRun>> g_engines;
+static std::map<std::tuple<aur_ctx*, uint32_t, int, int, int>, std::unique_ptr<WfRun>> g_engines;
 
 static WfRun* engine_for(aur_ctx* ctx, const WfConfig& cfg, int nscenes, cudaError_t* err) {
     std::lock_guard<std::mutex> lock(g_engine_mutex);
-    const auto key = std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort);
+    const auto key = std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort, cfg.record);
     auto it = g_engines.find(key);
     if (it != g_engines.end() && it->second->cap_scenes >= nscenes) return it->second.get();
     if (it != g_engines.end()) { it->second->release(); g_engines.erase(it); }
@@ -805,7 +830,7 @@ static WfRun* engine_for(aur_ctx* ctx, const WfConfig& cfg, int nscenes, cudaErr
 
 static void wf_drop_engine(aur_ctx* ctx, const WfConfig& cfg) {
     std::lock_guard<std::mutex> lock(g_engine_mutex);
-    auto it = g_engines.find(std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort));
+    auto it = g_engines.find(std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort, cfg.record));
     if (it != g_engines.end()) { it->second->release(); g_engines.erase(it); }
 }
 
@@ -909,6 +934,47 @@ static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, c
         stats->wf_block = cfg.block;
         stats->wf_sort = cfg.sort;
     }
+    return AUR_OK;
+}
+
+// Record pass of the path-replay adjoint: traces samples [s0, s0 + nsamples) of every
+// pixel with the wavefront engine in record mode and writes, per item (sample-major:
+// sl * npix + pixel), the hit records of its vertices (p.max_depth slots) and its
+// unclamped radiance. Ordered after the caller's stream and before its later work.
+aur_status wf_record_pass(aur_scene* sc, const PathParams& p, int s0, int nsamples, float4* rec, float4* lo_raw,
+                          uint64_t* launches, unsigned long long* rays) {
+    aur_ctx* ctx = sc->ctx;
+    WfConfig cfg;
+    if (sc->wf_tuned) { cfg.pool = (uint32_t)sc->wf_pool; cfg.block = sc->wf_block; cfg.sort = sc->wf_sort; }
+    cfg.record = 1;
+    cudaStream_t s = ctx->work_stream;
+    cudaEventRecord(ctx->ev_order, ctx->stream);
+    cudaStreamWaitEvent(s, ctx->ev_order, 0);
+    cudaError_t e = cudaSuccess;
+    WfRun* engine = engine_for(ctx, cfg, 1, &e);
+    if (!engine) return cuda_fail(e, "adjoint record pass: pool allocation");
+    WfRun& run = *engine;
+    std::vector<BatchItem> items(1);
+    items[0] = {sc, p, (uint32_t)sc->cam.w * (uint32_t)sc->cam.h, nullptr, nullptr};
+    std::vector<WfScene> tab;
+    const uint32_t total = fill_table(items, s0, nsamples, nullptr, tab, run.cap_scenes);
+    tab[0].rec = rec;
+    tab[0].lo_raw = lo_raw;
+    tab[0].rec_depth = (uint32_t)p.max_depth;
+    e = cudaMemsetAsync(run.w.rays, 0, 2 * sizeof(unsigned long long), s);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(run.d_scenes, tab.data(), sizeof(WfScene) * run.cap_scenes, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = run.run_pass(total, launches);
+    unsigned long long r[2] = {0, 0};
+    if (e == cudaSuccess) e = cudaMemcpyAsync(r, run.w.rays, sizeof(r), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // the host table and counters are read back
+    cudaEventRecord(ctx->ev_order, s);
+    cudaStreamWaitEvent(ctx->stream, ctx->ev_order, 0);
+    if (e != cudaSuccess) wf_drop_engine(ctx, cfg);
+    if (e == cudaErrorLaunchTimeout) return fail(AUR_ERR_TIMEOUT, "adjoint record pass: the path pool did not drain");
+    if (e != cudaSuccess) return cuda_fail(e, "adjoint record pass");
+    rays[0] += r[0];
+    rays[1] += r[1];
     return AUR_OK;
 }
 

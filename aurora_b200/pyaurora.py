@@ -25,7 +25,7 @@ def _opts(o: dict, adjoint: bool = False):
     spp = int(o.get("adjoint_spp", o["spp"]) if adjoint else o["spp"])
     depth = int(o["max_depth"])
     return render_opts(spp, depth, int(o.get("min_depth", depth)), int(o.get("seed", 0)),
-                       mode=_MODES[o.get("mode", "wavefront")] if not adjoint else _abi.RENDER_PLAIN,
+                       mode=_MODES[o.get("mode", "wavefront")],
                        sample_offset=int(o.get("sample_offset", 0)))
 
 
@@ -43,7 +43,8 @@ class AuroraRender(torch.autograd.Function):
     """image = AuroraRender.apply(mat_params (nmat, 4), texels (ntexel,), scene, options).
 
     Forward renders with the given per-material (diffuse rgb, roughness) and texels;
-    backward runs the path-replay adjoint with the same random numbers. options:
+    backward runs the path-replay adjoint with the same random numbers (wavefront mode: record
+    pass on the wavefront engine + replay kernel; plain mode: one megakernel). options:
     spp, max_depth, min_depth, seed, mode ("wavefront" | "plain"), adjoint_spp.
     """
 

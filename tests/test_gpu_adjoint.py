@@ -25,9 +25,9 @@ def loss(scene, params, texels, w, spp, seed=2):
     return float(np.sum(film.astype(np.float64) * w))
 
 
-def adjoint(scene, w, spp, seed=2):
+def adjoint(scene, w, spp, seed=2, mode=0):
     import aurora_b200 as ab
-    gm, gt, stats = scene.adjoint(ab.render_opts(spp, 6, 6, seed), w)
+    gm, gt, stats = scene.adjoint(ab.render_opts(spp, 6, 6, seed, mode=mode), w)
     return gm.astype(np.float64), gt.astype(np.float64), stats
 
 
@@ -99,14 +99,27 @@ def test_autograd_function(ctx):
     img = AuroraRender.apply(params, texels, scene, opts)
     wt = torch.tensor(w, device="cuda")
     (img * wt).sum().backward()
-    gm, gt, _ = adjoint(scene, w, 8)
+    gm, gt, _ = adjoint(scene, w, 8, mode=1)     # the binding's default mode is wavefront
     np.testing.assert_allclose(params.grad.cpu().numpy(), gm, rtol=1e-5, atol=1e-6)
     np.testing.assert_allclose(texels.grad.cpu().numpy(), gt, rtol=1e-5, atol=1e-6)
     assert img.shape == (32, 32, 4)
 
 
-def test_adjoint_is_deterministic(ctx):
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_adjoint_is_deterministic(ctx, mode):
     data, scene, w = setup(ctx, res=32)
-    a = adjoint(scene, w, 8)
-    b = adjoint(scene, w, 8)
+    a = adjoint(scene, w, 8, mode=mode)
+    b = adjoint(scene, w, 8, mode=mode)
     assert np.allclose(a[0], b[0], rtol=1e-5, atol=1e-7) and np.allclose(a[1], b[1], rtol=1e-5, atol=1e-7)
+
+
+def test_wavefront_adjoint_equals_plain_adjoint(ctx):
+    """Record pass on the wavefront engine + replay kernel against the megakernel: the same
+    paths and the same per-vertex arithmetic, summed in a different order."""
+    data, scene, w = setup(ctx, res=48)
+    a = adjoint(scene, w, 16, mode=0)
+    b = adjoint(scene, w, 16, mode=1)
+    assert b[2]["launches"] > 2 and b[2]["closest_rays"] == a[2]["closest_rays"]
+    assert b[2]["shadow_rays"] == a[2]["shadow_rays"]
+    for x, y in ((a[0], b[0]), (a[1], b[1])):
+        np.testing.assert_allclose(y, x, rtol=1e-4, atol=1e-5 * float(np.max(np.abs(x))))

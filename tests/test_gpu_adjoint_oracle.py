@@ -23,7 +23,7 @@ def _compare(gpu, cpu, what):
     assert np.all(err <= bound), what
 
 
-def _run(ctx, kelemen_tables, oracle_lib, data, crop, spp, seed, wseed):
+def _run(ctx, kelemen_tables, oracle_lib, data, crop, spp, seed, wseed, mode):
     import aurora_b200 as ab
     H, W = data.height, data.width
     w = np.zeros((H, W, 4), np.float32)
@@ -31,29 +31,31 @@ def _run(ctx, kelemen_tables, oracle_lib, data, crop, spp, seed, wseed):
     w[y0:y0 + ch, x0:x0 + cw, :3] = np.random.default_rng(wseed).normal(size=(ch, cw, 3))
     depth, mind = data.render["max_depth"], data.render["min_depth"]
     scene = ab.Scene(ctx, data)
-    gm, gt, _ = scene.adjoint(ab.render_opts(spp, depth, mind, seed), w)
+    gm, gt, _ = scene.adjoint(ab.render_opts(spp, depth, mind, seed, mode=mode), w)
     scene.close()
     osc = oracle_lib.OracleScene(data, kelemen_tables, use_bvh=True)
     cm, ct = osc.adjoint(spp, depth, mind, seed, w, crop=crop)
     return gm, gt, cm, ct
 
 
-def test_adjoint_matches_fp64_oracle_texture_scene(ctx, kelemen_tables, oracle_lib):
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_adjoint_matches_fp64_oracle_texture_scene(ctx, kelemen_tables, oracle_lib, mode):
     """Differentiable workload at 256x256: Kelemen sphere (diffuse + roughness with the lobe
     score term) over the textured ground (texel gradients)."""
     from aurora_b200 import scenes
     data = scenes.texture_scene()
-    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (112, 180, 32, 32), 64, 2, 21)
+    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (112, 180, 32, 32), 64, 2, 21, mode)
     assert np.count_nonzero(ct) > 100 and cm[1, 3] != 0.0
     _compare(gm, cm, "materials (diffuse rgb, roughness)")
     _compare(gt, ct, "texels")
 
 
-def test_adjoint_matches_fp64_oracle_cook_torrance(ctx, kelemen_tables, oracle_lib):
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_adjoint_matches_fp64_oracle_cook_torrance(ctx, kelemen_tables, oracle_lib, mode):
     """Box workload: Cook-Torrance boxes (roughness through eval, MIS and sampled lobes) and
     Lambert walls."""
     from aurora_b200 import scenes
     data = scenes.box_scene(128, 128, spp=64)
-    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (40, 72, 32, 32), 64, 1, 22)
+    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (40, 72, 32, 32), 64, 1, 22, mode)
     assert cm[3, 3] != 0.0
     _compare(gm, cm, "materials (diffuse rgb, roughness)")
