@@ -103,10 +103,14 @@ class Clocks:
 
 
 def render_opts_for(data, mode, rank=0, count_work=0, spp=None):
+    """Options of one step on `rank`: the full frame with the rank's own sample range
+    [rank * spp, (rank + 1) * spp) (weak scaling, no data-path collective)."""
     import aurora_b200 as ab
+    from aurora_b200.shard import sample_range
     r = data.render
     s = spp or r["spp"]
-    return ab.render_opts(s, r["max_depth"], r["min_depth"], r["seed"], mode=mode, sample_offset=rank * s,
+    first, count = sample_range(rank, rank + 1, s, "weak")
+    return ab.render_opts(count, r["max_depth"], r["min_depth"], r["seed"], mode=mode, sample_offset=first,
                           count_work=count_work)
 
 
@@ -249,6 +253,7 @@ def main():
     import torch
     import aurora_b200 as ab
     from aurora_b200 import _abi
+    from aurora_b200.shard import max_over_ranks
 
     rank, world = int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -302,9 +307,8 @@ def main():
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         if dist:
-            t = torch.tensor([ms, kernel_ms], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms, kernel_ms = float(t[0]), float(t[1])
+            ms = max_over_ranks(ms, device="cuda")
+            kernel_ms = max_over_ranks(kernel_ms, device="cuda")
         return ms / steps, kernel_ms / steps, launches, stats
 
     # headline mode, with clocks sampled during the timed region
@@ -379,9 +383,7 @@ def main():
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / e2e_steps
         if dist:
-            t = torch.tensor([dt], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            dt = float(t[0])
+            dt = max_over_ranks(dt, device="cuda")
         e2e = {"value": world * paths_step / dt, "unit": "path samples/s", "h2d_bytes_per_step": int(desc_bytes),
                "d2h_bytes_per_step": int(host_film.nbytes), "ms_per_step": dt * 1000,
                "includes": "scene upload + device BVH build + render + film download"}
