@@ -27,6 +27,7 @@ STATUS_NAMES = {0: "AUR_OK", 1: "AUR_ERR_INVALID_ARG", 2: "AUR_ERR_OOM", 3: "AUR
 
 MAT_MATTE, MAT_KELEMEN, MAT_COOKTORRANCE, MAT_METAL, MAT_CONSTANT = 0, 1, 2, 3, 4
 LIGHT_SQUARE, LIGHT_SPHERE = 0, 1
+ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_QUEUE_OVERFLOW, ERR_PARSE, ERR_IO, ERR_UNSUPPORTED = range(1, 9)
 RENDER_PLAIN, RENDER_WAVEFRONT = 0, 1
 
 f3 = C.c_float * 3
@@ -99,7 +100,12 @@ SIGNATURES = {
     "aur_trace_closest": (st, [vp, vp, vp, C.c_uint32]),
     "aur_trace_occluded": (st, [vp, vp, vp, C.c_uint32]),
     "aur_scene_create": (st, [vp, C.POINTER(SceneDesc), C.POINTER(BvhOpts), pp]),
-    "aur_scene_load_json": (st, [vp, C.c_char_p, pp]),
+    "aur_scene_load_json": (st, [vp, C.c_char_p, C.POINTER(BvhOpts), pp, C.POINTER(RenderOpts)]),
+    "aur_scene_file_read": (st, [C.c_char_p, pp]),
+    "aur_scene_file_desc": (st, [vp, C.POINTER(SceneDesc), C.POINTER(RenderOpts)]),
+    "aur_scene_file_output": (C.c_char_p, [vp]),
+    "aur_scene_file_light_samples": (C.c_int32, [vp]),
+    "aur_scene_file_destroy": (st, [vp]),
     "aur_scene_destroy": (st, [vp]),
     "aur_scene_info": (st, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
                             C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),

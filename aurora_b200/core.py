@@ -149,8 +149,12 @@ class Scene:
     def __init__(self, ctx: Context, data=None, bvh: _abi.BvhOpts | None = None, json_path: str | None = None):
         self.ctx = ctx
         h = C.c_void_p()
+        self.file_opts = None
         if json_path is not None:
-            check(lib().aur_scene_load_json(ctx.handle, json_path.encode(), C.byref(h)), "aur_scene_load_json")
+            o = _abi.RenderOpts()
+            check(lib().aur_scene_load_json(ctx.handle, json_path.encode(), C.byref(bvh) if bvh else None, C.byref(h),
+                                            C.byref(o)), "aur_scene_load_json")
+            self.file_opts = o    # render options from the file's "options"
         else:
             desc = data.desc()
             check(lib().aur_scene_create(ctx.handle, C.byref(desc), C.byref(bvh) if bvh else None, C.byref(h)),

@@ -117,7 +117,7 @@ namespace aur {
 // Traversal stack of one thread: the first kSharedDepth entries live in shared
 // memory laid out [depth][thread] (consecutive threads hit consecutive banks at
 // any mix of depths, one wavefront per warp access), deeper entries in local memory.
-constexpr int kSharedDepth = 24;
+constexpr int kSharedDepth = 24;   // all-local stacks measured 1.7% slower in k_extend
 struct LaneStack {
     int* col;                       // &s_stack[threadIdx.x]
     int stride;                     // blockDim.x

@@ -17,6 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import math
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -311,6 +312,51 @@ class SceneBuilder:
                          np.concatenate(attr), np.concatenate(cn).astype(F32), np.concatenate(cu).astype(F32),
                          attr_mat, attr_em, materials, [l[0] for l in self.lights], list(self.textures),
                          self.fov, self.width, self.height, self.name, dict(render or {}))
+
+
+def load_scene_file(path: str):
+    """Reads a scene file of the reference's JSON schema (options, renderCam, shaders,
+    materials, objects with OBJ meshes and square lights) with the library's host-side
+    loader (aur_scene_file_read; no device work). Returns (SceneData, RenderOpts, info)
+    where info holds the file's output name and light-sample count."""
+    h = C.c_void_p()
+    _abi.check(_abi.lib().aur_scene_file_read(path.encode(), C.byref(h)), "aur_scene_file_read")
+    try:
+        d = _abi.SceneDesc()
+        o = _abi.RenderOpts()
+        _abi.check(_abi.lib().aur_scene_file_desc(h, C.byref(d), C.byref(o)), "aur_scene_file_desc")
+
+        def arr(ptr, n, dtype, shape):
+            if n == 0 or not ptr:
+                return np.zeros([0 if x == -1 else x for x in shape], dtype)
+            ct = {np.float32: C.c_float, np.uint32: C.c_uint32, np.int32: C.c_int32}[dtype]
+            return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(n,)).copy().reshape(shape)
+        verts = arr(d.verts, 3 * d.nvert, np.float32, (d.nvert, 3))
+        vidx = arr(d.tri_vidx, 3 * d.ntri, np.uint32, (d.ntri, 3))
+        tattr = arr(d.tri_attr, d.ntri, np.int32, (d.ntri,))
+        cn = arr(d.corner_normals, 9 * d.ntri, np.float32, (d.ntri, 9))
+        cu = arr(d.corner_uvs, 6 * d.ntri, np.float32, (d.ntri, 6))
+        amat = arr(d.attr_material, d.nattr, np.int32, (d.nattr,))
+        aem = arr(d.attr_emission, 3 * d.nattr, np.float32, (d.nattr, 3))
+        mats = [_abi.MaterialDesc.from_buffer_copy(C.cast(d.materials, C.POINTER(_abi.MaterialDesc))[i])
+                for i in range(d.nmat)]
+        lights = [_abi.LightDesc.from_buffer_copy(C.cast(d.lights, C.POINTER(_abi.LightDesc))[i])
+                  for i in range(d.nlight)]
+        dims = arr(d.tex_dims, 2 * d.ntex, np.int32, (d.ntex, 2))
+        texels = arr(d.texels, int(3 * (dims[:, 0] * dims[:, 1]).sum()) if d.ntex else 0, np.float32, (-1,))
+        textures, off = [], 0
+        for w_, h_ in dims:
+            n = 3 * int(w_) * int(h_)
+            textures.append(texels[off:off + n].reshape(int(h_), int(w_), 3))
+            off += n
+        info = {"output": _abi.lib().aur_scene_file_output(h).decode(),
+                "light_samples": int(_abi.lib().aur_scene_file_light_samples(h))}
+        data = SceneData(verts, vidx, tattr, cn, cu, amat, aem, mats, lights, textures, float(d.fov), int(d.width),
+                         int(d.height), os.path.basename(path),
+                         dict(spp=o.spp, max_depth=o.max_depth, min_depth=o.min_depth, seed=0))
+        return data, o, info
+    finally:
+        _abi.lib().aur_scene_file_destroy(h)
 
 
 FOV40 = math.tan(math.radians(20.0))

@@ -173,8 +173,6 @@ typedef struct aur_scene_desc {
 
 AUR_API aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* desc, const aur_bvh_opts* bvh_opts,
                             aur_scene** out);
-/* Reference scene file (JSON schema of Aurora/src/translator/jsonParser.cpp:30-661). */
-AUR_API aur_status aur_scene_load_json(aur_ctx* ctx, const char* path, aur_scene** out);
 AUR_API aur_status aur_scene_destroy(aur_scene* scene);
 AUR_API aur_status aur_scene_info(const aur_scene* scene, int32_t* width, int32_t* height, uint32_t* ntri,
                           uint32_t* nmat, uint32_t* ntexel_floats);
@@ -205,6 +203,31 @@ typedef struct aur_render_opts {
     int32_t wf_sort;        /* wavefront material sort: -1 tuned, 0 off, 1 on */
     int32_t count_work;     /* also count BVH node visits / triangle tests (slower; for profiling) */
 } aur_render_opts;
+
+/* ------------------------------------------------------------ scene files
+ * Reference scene file: the JSON schema read by JsonParser
+ * (Aurora/src/translator/jsonParser.cpp:30-661) — options, renderCam, shaders
+ * (texture2DShader; texture files in PFM, EXR needs OpenEXR), materials
+ * (matteMaterial, kelemenMaterial, metalMaterial), objects (geometry: OBJ
+ * triangles with optional Loop subdivision, objTriangleMesh.cpp:26-92 and
+ * loopSubdivMesh.cpp:167-744; light: square lights). Relative paths resolve
+ * against the file's directory. glassMaterial, environment lights, normal maps
+ * and triplanar shaders return AUR_ERR_UNSUPPORTED.
+ * aur_scene_file_read flattens the file on the host (no device work) into
+ * arrays owned by the aur_scene_file; aur_scene_file_desc points a scene
+ * description at them and fills *opts (may be NULL) from "options"
+ * (pixelsamples -> spp, mindepth, maxdepth; mode wavefront, autotuned).
+ * aur_scene_load_json = read + aur_scene_create. */
+typedef struct aur_scene_file aur_scene_file;
+AUR_API aur_status aur_scene_file_read(const char* path, aur_scene_file** out);
+AUR_API aur_status aur_scene_file_desc(const aur_scene_file* file, aur_scene_desc* desc, aur_render_opts* opts);
+/* "options.filename" of the file (the reference's output image name). */
+AUR_API const char* aur_scene_file_output(const aur_scene_file* file);
+/* "options.lightsamples" of the file; the path traces one light sample per vertex. */
+AUR_API int32_t aur_scene_file_light_samples(const aur_scene_file* file);
+AUR_API aur_status aur_scene_file_destroy(aur_scene_file* file);
+AUR_API aur_status aur_scene_load_json(aur_ctx* ctx, const char* path, const aur_bvh_opts* bvh_opts,
+                                       aur_scene** out, aur_render_opts* opts);
 
 typedef struct aur_render_stats {
     uint64_t camera_rays;
