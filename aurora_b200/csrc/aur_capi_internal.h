@@ -19,6 +19,8 @@ struct aur_ctx {
     std::map<uint64_t, std::array<int, 3>> wf_batch_tuned;   // autotuned batch configs (pool, block, sort)
     std::map<uint64_t, std::array<int, 3>> wf_scene_tuned;   // autotuned configs by scene signature
     int live = 0;                              // BVHs and scenes created on this context and not destroyed
+    void* scratch = nullptr;                   // grow-only device scratch (adjoint hit records)
+    size_t scratch_bytes = 0;
 };
 
 struct aur_bvh {
@@ -57,6 +59,9 @@ aur_status fail(aur_status s, const std::string& msg);
 aur_status cuda_fail(cudaError_t e, const char* where);
 bool is_device_ptr(const void* p);
 cudaError_t ctx_kelemen_ensure(aur_ctx* ctx, int refl_index);
+// The context's scratch buffer of at least `bytes` (kept and reused by later calls;
+// freed with the context). Work on the context's stream must not still use it.
+cudaError_t ctx_scratch(aur_ctx* ctx, size_t bytes, void** out);
 int kelemen_index(float reflectance);
 aur_status bvh_options(const aur_bvh_opts* o, BvhBuildOptions* out);
 aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathParams* p);

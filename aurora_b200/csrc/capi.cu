@@ -76,6 +76,21 @@ cudaError_t ctx_kelemen_tables(aur_ctx* ctx) {
     }
     return cudaSuccess;
 }
+cudaError_t ctx_scratch(aur_ctx* ctx, size_t bytes, void** out) {
+    if (bytes > ctx->scratch_bytes) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);   // the old buffer may still be in use
+        if (e != cudaSuccess) return e;
+        if (ctx->scratch) cudaFree(ctx->scratch);
+        ctx->scratch = nullptr;
+        ctx->scratch_bytes = 0;
+        e = cudaMalloc(&ctx->scratch, bytes);
+        if (e != cudaSuccess) return e;
+        ctx->scratch_bytes = bytes;
+    }
+    *out = ctx->scratch;
+    return cudaSuccess;
+}
+
 cudaError_t ctx_kelemen_ensure(aur_ctx* ctx, int refl_index) {
     cudaError_t e = ctx_kelemen_tables(ctx);
     if (e != cudaSuccess) return e;
@@ -139,6 +154,7 @@ aur_status aur_ctx_create(int device, aur_ctx** out) {
     return AUR_OK;
 }
 
+
 aur_status aur_ctx_destroy(aur_ctx* ctx) {
     if (!ctx) return AUR_OK;
     if (ctx->live > 0)
@@ -147,6 +163,7 @@ aur_status aur_ctx_destroy(aur_ctx* ctx) {
     cudaStreamSynchronize(ctx->stream);
     wf_release_context(ctx);
     if (ctx->kelemen) cudaFree(ctx->kelemen);
+    if (ctx->scratch) cudaFree(ctx->scratch);
     if (ctx->counters) cudaFree(ctx->counters);
     if (ctx->work_stream) { cudaStreamSynchronize(ctx->work_stream); cudaStreamDestroy(ctx->work_stream); }
     if (ctx->ev_order) cudaEventDestroy(ctx->ev_order);

@@ -175,11 +175,16 @@ def adjoint_ratio(ab, _abi, torch, ctx, stream, steps=2, warmup=1):
         return lambda: sc.adjoint(ab.render_opts(spp, depth, depth, data.render["seed"], mode=mode), dfilm, gm, gt)
 
     a_wf = dev_ms(adj(_abi.RENDER_WAVEFRONT))
+    st = sc.adjoint(ab.render_opts(spp, depth, depth, data.render["seed"], mode=_abi.RENDER_WAVEFRONT), dfilm, gm,
+                    gt)[2]
+    split = {"record_ms": st["stage_ms"]["regen"], "replay_ms": st["stage_ms"]["extend"],
+             "wavefront_config": st["wf_config"]}
     a_plain = dev_ms(adj(_abi.RENDER_PLAIN))
     sc.close()
     return {"workload": f"texture {data.ntri} tris {W}x{H} {spp}spp depth {depth}, 16 materials + 64x64x3 texels",
             "forward_ms": f_wf, "adjoint_ms": a_wf, "ratio": a_wf / f_wf,
             "forward_plain_ms": f_plain, "adjoint_plain_ms": a_plain, "ratio_plain": a_plain / f_plain,
+            "adjoint_split": split,
             "note": "ratio: wavefront adjoint (record pass on the wavefront engine + replay kernel) over the "
                     "wavefront forward (the autograd pair); ratio_plain: megakernel adjoint over the plain forward"}
 
