@@ -1,0 +1,58 @@
+"""The device path against the committed golden vectors of the oracle
+(tests/golden/golden.npz): hit ids bit-exact, shading within 1e-5 relative, the image
+within 3 sigma of the oracle's mean, the adjoint within 1e-3 of the FP64 gradient."""
+import os
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.npz")
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return dict(np.load(GOLDEN))
+
+
+def test_hits_against_golden(ctx, golden):
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    sphere = scenes.sphere_scene(64, 64)
+    bvh = ab.Bvh(ctx, sphere.verts, sphere.tri_vidx, sphere.tri_attr)
+    hits = bvh.trace_closest(golden["ray_in"])
+    ok = golden["hit_ties"] <= 1
+    np.testing.assert_array_equal(hits["prim"][ok], golden["hit_prim"][ok])
+    hit = ok & (golden["hit_prim"] >= 0)
+    got = np.stack([hits["t"], hits["u"], hits["v"]], 1)
+    np.testing.assert_array_equal(got[hit], golden["hit_tuv"][hit])
+    bvh.close()
+
+
+def test_shading_against_golden(ctx, golden):
+    ev, sm = golden["brdf_eval_in"], golden["brdf_sample_in"]
+    for kind, inp, ref in ((1, ev, golden["brdf_eval_out"]), (2, ev, golden["brdf_pdf_out"]),
+                           (0, sm, golden["brdf_sample_out"])):
+        got = ctx.probe(kind, inp)
+        bad = np.abs(got - ref) > 1e-7 + 1e-5 * np.abs(ref)
+        assert np.any(bad.reshape(len(ref), -1), axis=1).mean() <= 0.002, kind
+
+
+def test_image_and_adjoint_against_golden(ctx, golden):
+    import aurora_b200 as ab
+    from aurora_b200 import _abi, scenes
+    box = scenes.box_scene(16, 16, spp=8)
+    scene = ab.Scene(ctx, box)
+    mean, m2 = golden["box_mean"], golden["box_m2"]
+    sig = np.sqrt(m2 / 7 / 8)
+    for mode in (_abi.RENDER_PLAIN, _abi.RENDER_WAVEFRONT):
+        film = scene.render(ab.render_opts(8, 5, 5, 1, mode=mode)).film
+        d = np.abs(film[..., :3] - mean[..., :3])
+        assert np.mean(d <= 3 * sig + 1e-5 * (1 + mean[..., :3])) > 0.995
+        np.testing.assert_array_equal(film[..., 3], mean[..., 3].astype(np.float32))
+    for mode in (_abi.RENDER_PLAIN, _abi.RENDER_WAVEFRONT):
+        gm, _, _ = scene.adjoint(ab.render_opts(8, 5, 5, 1, mode=mode), golden["box_dfilm"])
+        ref = golden["box_grad"]
+        np.testing.assert_allclose(gm, ref, rtol=1e-3, atol=1e-4 * np.abs(ref).max())
+    scene.close()
