@@ -13,7 +13,7 @@
 //           continuation, throughput and roulette -> next extension queue
 //   shadow  occlusion for the next-event rays, Lo += direct * T
 //
-// Queues are compacted with warp ballots (one atomic per warp). Many scenes of
+// Queue appends and work fetches are aggregated per block (one atomic per block). Many scenes of
 // different resolution, spp and depth share one pool (batched launch). The
 // per-iteration kernels are captured once into a CUDA graph and replayed.
 // Every (pixel, sample) result goes to a per-sample buffer and is resolved in
@@ -83,22 +83,30 @@ __device__ __forceinline__ bool f_matte(uint32_t f) { return (f >> 20) & 1; }
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31; }
 __device__ __forceinline__ uint32_t lanemask_lt() { return (1u << lane_id()) - 1u; }
 
-// Warp-aggregated append: lanes with `pred` get consecutive slots of `q`.
-__device__ __forceinline__ void warp_push(bool pred, uint32_t value, uint32_t* q, uint32_t* count) {
-    const uint32_t m = __ballot_sync(0xffffffffu, pred);
-    if (!m) return;
-    uint32_t base = 0;
-    const int leader = __ffs(m) - 1;
-    if ((int)lane_id() == leader) base = atomicAdd(count, (uint32_t)__popc(m));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    if (pred) q[base + __popc(m & lanemask_lt())] = value;
-}
-
-// Persistent-warp fetch: returns the first index of the warp's next batch of 32.
-__device__ __forceinline__ uint32_t warp_fetch(uint32_t* cursor) {
-    uint32_t b = 0;
-    if (lane_id() == 0) b = atomicAdd(cursor, 32u);
-    return __shfl_sync(0xffffffffu, b, 0);
+// Block-aggregated append to up to three queues: every thread of the block calls it
+// (uniform control flow) with its flags; it returns each flagged thread's slot in the
+// queue. One atomic per queue per block instead of one per warp.
+struct BlockScan { uint32_t cnt[16][3]; uint32_t base[3]; };
+__device__ __forceinline__ void block_reserve(BlockScan& sh, const bool (&p)[3], uint32_t* const (&ctr)[3],
+                                              uint32_t (&pos)[3]) {
+    const int warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    uint32_t m[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) m[q] = __ballot_sync(0xffffffffu, p[q]);
+    if (lane_id() == 0)
+#pragma unroll
+        for (int q = 0; q < 3; ++q) sh.cnt[warp][q] = __popc(m[q]);
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        const int q = threadIdx.x;
+        uint32_t t = 0;
+        for (int j = 0; j < nw; ++j) { const uint32_t c = sh.cnt[j][q]; sh.cnt[j][q] = t; t += c; }
+        sh.base[q] = (t && ctr[q]) ? atomicAdd(ctr[q], t) : 0u;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 3; ++q) pos[q] = sh.base[q] + sh.cnt[warp][q] + __popc(m[q] & lanemask_lt());
+    __syncthreads();   // sh is reused by the next call
 }
 
 __device__ __forceinline__ int scene_of(const WfPool& w, uint32_t item) {
@@ -113,6 +121,7 @@ __device__ __forceinline__ int scene_of(const WfPool& w, uint32_t item) {
 // ------------------------------------------------------------------ regen
 template <bool kRec>
 __global__ void k_regen(WfPool w, int in_q) {
+    __shared__ BlockScan s_scan;
     uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
     uint32_t* cin = &w.ctr[in_q ? C_EXT1 : C_EXT0];
     const uint32_t total = w.ctr[C_TOTAL];
@@ -153,14 +162,13 @@ __global__ void k_regen(WfPool w, int in_q) {
             st = PS_EMPTY;
         }
         const bool want = st == PS_EMPTY && *(volatile uint32_t*)&w.ctr[C_WORK] < total;
-        const uint32_t m = __ballot_sync(0xffffffffu, want);
         uint32_t item = 0xffffffffu;
-        if (m) {
-            uint32_t b = 0;
-            const int leader = __ffs(m) - 1;
-            if ((int)lane_id() == leader) b = atomicAdd(&w.ctr[C_WORK], (uint32_t)__popc(m));
-            b = __shfl_sync(0xffffffffu, b, leader);
-            if (want) item = b + __popc(m & lanemask_lt());
+        {
+            const bool pw[3] = {want, false, false};
+            uint32_t* const cw[3] = {&w.ctr[C_WORK], nullptr, nullptr};
+            uint32_t pos[3];
+            block_reserve(s_scan, pw, cw, pos);
+            if (want) item = pos[0];
         }
         const bool start = want && item < total;
         if (start) {
@@ -180,7 +188,13 @@ __global__ void k_regen(WfPool w, int in_q) {
             w.id[i] = make_uint4((uint32_t)s, pixel, sl, pack_flags(0, 0, RAY_CAMERA, false));
             st = PS_ACTIVE;
         }
-        warp_push(start, i, qin, cin);
+        {
+            const bool pp[3] = {start, false, false};
+            uint32_t* const cp[3] = {cin, nullptr, nullptr};
+            uint32_t pos[3];
+            block_reserve(s_scan, pp, cp, pos);
+            if (start) qin[pos[0]] = i;
+        }
         if (valid) w.state[i] = st;
     }
 }
@@ -212,6 +226,9 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
         w.rays[0] += n;
     }
     extern __shared__ int s_stack[];
+    __shared__ uint32_t s_bucket[kBuckets];   // per-block material counts, added to the global ones at exit
+    if (kSort && threadIdx.x < kBuckets) s_bucket[threadIdx.x] = 0;
+    __syncthreads();
     LaneStack stack;
     stack.col = s_stack + threadIdx.x;
     stack.stride = blockDim.x;
@@ -257,13 +274,17 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
             if (kSort) bucket = bucket_of(S->sc.sh, ts.best);
             has = false;
         }
-        if (kSort) {   // per-bucket counts, one atomic per (warp, bucket)
+        if (kSort) {   // per-bucket counts, one shared atomic per (warp, bucket)
             const uint32_t fin = __ballot_sync(0xffffffffu, bucket >= 0);
             if (bucket >= 0) {
                 const uint32_t peers = __match_any_sync(fin, bucket);
-                if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&w.ctr[C_BUCKET + bucket], (uint32_t)__popc(peers));
+                if ((int)lane_id() == __ffs(peers) - 1) atomicAdd(&s_bucket[bucket], (uint32_t)__popc(peers));
             }
         }
+    }
+    if (kSort) {
+        __syncthreads();
+        if (threadIdx.x < kBuckets && s_bucket[threadIdx.x]) atomicAdd(&w.ctr[C_BUCKET + threadIdx.x], s_bucket[threadIdx.x]);
     }
 }
 
@@ -271,18 +292,21 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
 __global__ void k_sort_scatter(WfPool w, int in_q) {
     const uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
     const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
-    __shared__ uint32_t s_ofs[kBuckets];
+    __shared__ uint32_t s_ofs[kBuckets], s_cnt[kBuckets], s_base[kBuckets];
+    __shared__ uint32_t s_fetch;
     if (threadIdx.x == 0) {
         uint32_t a = 0;
         for (int b = 0; b < kBuckets; ++b) { s_ofs[b] = a; a += w.ctr[C_BUCKET + b]; }
     }
-    __syncthreads();
-    while (true) {
-        const uint32_t b = warp_fetch(&w.ctr[C_CUR_SORT]);
+    while (true) {   // a block takes blockDim entries at a time; one atomic per bucket per block
+        if (threadIdx.x == 0) s_fetch = atomicAdd(&w.ctr[C_CUR_SORT], blockDim.x);
+        if (threadIdx.x < kBuckets) s_cnt[threadIdx.x] = 0;
+        __syncthreads();
+        const uint32_t b = s_fetch;
         if (b >= n) break;
-        const uint32_t k = b + lane_id();
+        const uint32_t k = b + threadIdx.x;
         int bucket = -1;
-        uint32_t slot = 0;
+        uint32_t slot = 0, local = 0;
         if (k < n) {
             slot = qin[k];
             const int prim = __float_as_int(w.hit[slot].w);
@@ -292,11 +316,16 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
         if (bucket >= 0) {
             const uint32_t peers = __match_any_sync(active, bucket);
             const int leader = __ffs(peers) - 1;
-            uint32_t base = 0;
-            if ((int)lane_id() == leader) base = atomicAdd(&w.ctr[C_FILL + bucket], (uint32_t)__popc(peers));
-            base = __shfl_sync(peers, base, leader);
-            w.q_sort[s_ofs[bucket] + base + __popc(peers & lanemask_lt())] = slot;
+            uint32_t wb = 0;
+            if ((int)lane_id() == leader) wb = atomicAdd(&s_cnt[bucket], (uint32_t)__popc(peers));
+            local = __shfl_sync(peers, wb, leader) + __popc(peers & lanemask_lt());
         }
+        __syncthreads();
+        if (threadIdx.x < kBuckets)
+            s_base[threadIdx.x] = s_cnt[threadIdx.x] ? atomicAdd(&w.ctr[C_FILL + threadIdx.x], s_cnt[threadIdx.x]) : 0u;
+        __syncthreads();
+        if (bucket >= 0) w.q_sort[s_ofs[bucket] + s_base[bucket] + local] = slot;
+        __syncthreads();   // s_fetch and s_cnt are rewritten next round
     }
 }
 
@@ -311,10 +340,14 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
         w.ctr[C_CUR_EXT] = 0;
         for (int k = 0; k < kBuckets; ++k) { w.ctr[C_BUCKET + k] = 0; w.ctr[C_FILL + k] = 0; }
     }
+    __shared__ BlockScan s_scan;
+    __shared__ uint32_t s_fetch;
     while (true) {
-        const uint32_t b = warp_fetch(&w.ctr[C_CUR_SHADE]);
+        if (threadIdx.x == 0) s_fetch = atomicAdd(&w.ctr[C_CUR_SHADE], blockDim.x);
+        __syncthreads();
+        const uint32_t b = s_fetch;   // rewritten only after block_reserve's barriers below
         if (b >= n) break;
-        const uint32_t k = b + lane_id();
+        const uint32_t k = b + threadIdx.x;
         bool push_ext = false, push_sh0 = false, push_sh1 = false;
         uint32_t slot = 0;
         if (k < n) {
@@ -441,9 +474,15 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
             }
             w.lo[slot] = lo;
         }
-        warp_push(push_ext, slot, qout, cout);
-        warp_push(push_sh0, slot << 1, w.q_shadow, &w.ctr[C_SHADOW]);
-        warp_push(push_sh1, (slot << 1) | 1u, w.q_shadow, &w.ctr[C_SHADOW]);
+        {
+            const bool pp[3] = {push_ext, push_sh0, push_sh1};
+            uint32_t* const cp[3] = {cout, &w.ctr[C_SHADOW], &w.ctr[C_SHADOW]};
+            uint32_t pos[3];
+            block_reserve(s_scan, pp, cp, pos);
+            if (push_ext) qout[pos[0]] = slot;
+            if (push_sh0) w.q_shadow[pos[1]] = slot << 1;
+            if (push_sh1) w.q_shadow[pos[2]] = (slot << 1) | 1u;
+        }
     }
 }
 
