@@ -6,7 +6,7 @@ package does not load the library; the first call that needs it does, and
 fails loudly if it has not been built.
 """
 from ._abi import AuroraError, lib  # noqa: F401
-from .core import Bvh, Context, RenderResult, Scene, render_batch, render_opts, bvh_opts  # noqa: F401
+from .core import Bvh, Context, RenderResult, Scene, render_batch, render_opts, bvh_opts, write_film  # noqa: F401
 
 __all__ = ["AuroraError", "Bvh", "Context", "Scene", "RenderResult", "render_batch", "render_opts", "bvh_opts",
-           "lib"]
+           "write_film", "lib"]

@@ -28,6 +28,7 @@ STATUS_NAMES = {0: "AUR_OK", 1: "AUR_ERR_INVALID_ARG", 2: "AUR_ERR_OOM", 3: "AUR
 MAT_MATTE, MAT_KELEMEN, MAT_COOKTORRANCE, MAT_METAL, MAT_CONSTANT = 0, 1, 2, 3, 4
 LIGHT_SQUARE, LIGHT_SPHERE = 0, 1
 ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_QUEUE_OVERFLOW, ERR_PARSE, ERR_IO, ERR_UNSUPPORTED = range(1, 9)
+FILM_PFM, FILM_EXR_HALF, FILM_EXR_FLOAT = 0, 1, 2
 RENDER_PLAIN, RENDER_WAVEFRONT = 0, 1
 
 f3 = C.c_float * 3
@@ -106,6 +107,7 @@ SIGNATURES = {
     "aur_scene_file_output": (C.c_char_p, [vp]),
     "aur_scene_file_light_samples": (C.c_int32, [vp]),
     "aur_scene_file_destroy": (st, [vp]),
+    "aur_film_write": (st, [C.c_char_p, vp, C.c_int32, C.c_int32, C.c_int32]),
     "aur_scene_destroy": (st, [vp]),
     "aur_scene_info": (st, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_uint32),
                             C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]),

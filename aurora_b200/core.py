@@ -218,6 +218,18 @@ class Scene:
         return gm, gt, _stats(s)
 
 
+def write_film(path: str, film, fmt: int = _abi.FILM_EXR_HALF) -> None:
+    """Writes an (H, W, 4) float32 film (numpy or CUDA tensor) as OpenEXR (half or float
+    RGBA, uncompressed) or PFM (RGB float)."""
+    if hasattr(film, "data_ptr"):
+        h, w = int(film.shape[0]), int(film.shape[1])
+        f = film.contiguous()
+    else:
+        f = np.ascontiguousarray(film, np.float32)
+        h, w = f.shape[:2]
+    check(lib().aur_film_write(path.encode(), _ptr(f), w, h, fmt), "aur_film_write")
+
+
 def render_batch(scenes: list[Scene], opts: list[_abi.RenderOpts], films=None):
     n = len(scenes)
     if films is None:

@@ -229,6 +229,14 @@ AUR_API aur_status aur_scene_file_destroy(aur_scene_file* file);
 AUR_API aur_status aur_scene_load_json(aur_ctx* ctx, const char* path, const aur_bvh_opts* bvh_opts,
                                        aur_scene** out, aur_render_opts* opts);
 
+/* Film output: a film of width*height RGBA floats (top row first; host or device
+ * memory) written as OpenEXR (the reference's output, OpenexrDisplay,
+ * frontend/openexrDisplay.cpp:132-244: RGBA, HALF or FLOAT channels, uncompressed
+ * scanlines) or PFM (RGB float, rows bottom to top). */
+enum { AUR_FILM_PFM = 0, AUR_FILM_EXR_HALF = 1, AUR_FILM_EXR_FLOAT = 2 };
+AUR_API aur_status aur_film_write(const char* path, const float* film_rgba, int32_t width, int32_t height,
+                                  int32_t format);
+
 typedef struct aur_render_stats {
     uint64_t camera_rays;
     uint64_t closest_rays;  /* including camera rays */
