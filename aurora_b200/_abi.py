@@ -25,7 +25,7 @@ AUR_OK = 0
 STATUS_NAMES = {0: "AUR_OK", 1: "AUR_ERR_INVALID_ARG", 2: "AUR_ERR_OOM", 3: "AUR_ERR_CUDA", 4: "AUR_ERR_TIMEOUT",
                 5: "AUR_ERR_QUEUE_OVERFLOW", 6: "AUR_ERR_PARSE", 7: "AUR_ERR_IO", 8: "AUR_ERR_UNSUPPORTED"}
 
-MAT_MATTE, MAT_KELEMEN, MAT_COOKTORRANCE, MAT_METAL, MAT_CONSTANT = 0, 1, 2, 3, 4
+MAT_MATTE, MAT_KELEMEN, MAT_COOKTORRANCE, MAT_METAL, MAT_CONSTANT, MAT_GLASS = 0, 1, 2, 3, 4, 5
 LIGHT_SQUARE, LIGHT_SPHERE = 0, 1
 ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_QUEUE_OVERFLOW, ERR_PARSE, ERR_IO, ERR_UNSUPPORTED = range(1, 9)
 FILM_PFM, FILM_EXR_HALF, FILM_EXR_FLOAT = 0, 1, 2
@@ -50,7 +50,8 @@ class BvhOpts(C.Structure):
 class MaterialDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("diffuse", f3), ("specular", f3), ("gain", f3), ("roughness", C.c_float),
                 ("roughness_b", C.c_float), ("reflectance", C.c_float), ("mix", C.c_float),
-                ("diffuse_tex", C.c_int32), ("specular_tex", C.c_int32), ("roughness_tex", C.c_int32)]
+                ("diffuse_tex", C.c_int32), ("specular_tex", C.c_int32), ("roughness_tex", C.c_int32),
+                ("ior", C.c_float)]
 
 
 class LightDesc(C.Structure):

@@ -305,7 +305,7 @@ __device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams
         const Frame f = hit_frame(sc.sh, prim, r.x, r.y, r.z, ray.o, ray.d, true);
         const Attr at = sc.sh.attrs[f.attr];
         if (kind == RAY_DIFFUSE) matte = true;
-        if (kind == RAY_CAMERA) collected += T * at.emission;
+        if (collects_emission(kind)) collected += T * at.emission;
         const float lobe_u = rng.u(vertex_dim(vtx, kDimLobe));
         const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte, lobe_u);
         const ParamRef pr = param_of(sc.sh, at.material, brdf, f, matte, lobe_u);
@@ -352,17 +352,7 @@ __device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams
             mc.template add<3>(pr.index, g.x + g.y + g.z, s_g, s_c);
         }
         // the forward update, identical to pass 1
-        if (!cont_ok) break;
-        const float cosl = dot(f.N, bs.dir);
-        T *= cdiv(bs.color * cosl, bs.pdf);
-        if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
-        if (is_black(T)) break;
-        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
-        if (bounces > p.min_depth) {
-            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
-            T = cdiv(T, cont);
-        }
-        ++bounces;
+        if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
         ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
     }
 }
@@ -416,7 +406,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         const Frame f = hit_frame(sc.sh, h.prim, h.t, h.u, h.v, ray.o, ray.d, true);
                         const Attr at = sc.sh.attrs[f.attr];
                         if (kind == RAY_DIFFUSE) matte = true;
-                        if (kind == RAY_CAMERA) Lo += T * at.emission;
+                        if (collects_emission(kind)) Lo += T * at.emission;
                         const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
                                                    rng.u(vertex_dim(vtx, kDimLobe)));
                         uint32_t vis = 0;
@@ -424,17 +414,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         rec[vtx] = pack_rec(h, vis);
                         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
-                        if (bs.pdf <= 0.f) break;
-                        const float cosl = dot(f.N, bs.dir);
-                        T *= cdiv(bs.color * cosl, bs.pdf);
-                        if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
-                        if (is_black(T)) break;
-                        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
-                        if (bounces > p.min_depth) {
-                            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
-                            T = cdiv(T, cont);
-                        }
-                        ++bounces;
+                        if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
                         if (vtx + 1 >= p.max_depth) break;
                         ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
                         ++rc.closest;

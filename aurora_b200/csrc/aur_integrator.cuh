@@ -95,7 +95,39 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
     return res * (float)nvis;
 }
 
-enum RayKind : int { RAY_CAMERA = 0, RAY_DIFFUSE = 1, RAY_SPECULAR = 2 };
+enum RayKind : int { RAY_CAMERA = 0, RAY_DIFFUSE = 1, RAY_SPECULAR = 2, RAY_MIRROR = 3 };
+
+// Emission is added at vertices reached by camera and mirror rays (integrator.cpp:184-187).
+__device__ __forceinline__ bool collects_emission(int kind) { return kind == RAY_CAMERA || kind == RAY_MIRROR; }
+
+// Continuation of Integrator::integrateCameraSample (integrator.cpp:202-243) after the
+// BRDF sample `bs` of `brdf`: throughput, roulette probability, ray kind, roulette and the
+// bounce count. Delta lobes (mirror, transmission) multiply by the sample colour only,
+// skip the black test and do not count as bounces for roulette. Returns false when the
+// path ends.
+__device__ __forceinline__ bool continue_path(const Brdf& brdf, const BrdfSample& bs, float3 N, int min_depth,
+                                              const PathRng& rng, int vtx, float3& T, float& cont, int& kind,
+                                              int& bounces) {
+    if (bs.pdf <= 0.f) return false;
+    const bool delta = brdf.lobe == LOBE_MIRROR || brdf.lobe == LOBE_TRANSMIT;
+    if (!delta) {
+        const float cosl = dot(N, bs.dir);
+        T *= cdiv(bs.color * cosl, bs.pdf);
+        if (bounces > min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
+        if (is_black(T)) return false;
+        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
+    } else {
+        T *= bs.color;
+        if (bounces > min_depth) cont *= lum(bs.color);
+        kind = RAY_MIRROR;
+    }
+    if (bounces > min_depth) {
+        if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) return false;
+        T = cdiv(T, cont);
+    }
+    if (!delta) ++bounces;
+    return true;
+}
 
 // Firefly filter (integrator.cpp:278-281). A non-finite estimate would never
 // leave the reference's loop; it is dropped (returned as black) instead, which
@@ -125,23 +157,13 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         const Frame f = hit_frame(sc.sh, h.prim, h.t, h.u, h.v, ray.o, ray.d, true);
         const Attr at = sc.sh.attrs[f.attr];
         if (kind == RAY_DIFFUSE) matte_path = true;
-        if (kind == RAY_CAMERA) Lo += T * at.emission;
+        if (collects_emission(kind)) Lo += T * at.emission;
         const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte_path,
                                    rng.u(vertex_dim(vtx, kDimLobe)));
         Lo += integrate_direct(sc, f, brdf, rng, vtx, rc) * T;
         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
-        if (bs.pdf <= 0.f) break;
-        const float cosl = dot(f.N, bs.dir);
-        T *= cdiv(bs.color * cosl, bs.pdf);
-        if (bounces > p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
-        if (is_black(T)) break;
-        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
-        if (bounces > p.min_depth) {
-            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) break;
-            T = cdiv(T, cont);
-        }
-        ++bounces;
+        if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
         if (vtx + 1 >= p.max_depth) break;   // the reference's unshaded last ray
         ray.o = f.P;
         ray.d = bs.dir;

@@ -22,8 +22,11 @@
 namespace aur {
 
 // ------------------------------------------------------------------ records
-enum MatType : int { MAT_MATTE = 0, MAT_KELEMEN = 1, MAT_COOKTORRANCE = 2, MAT_METAL = 3, MAT_CONSTANT = 4 };
-enum LobeType : int { LOBE_MATTE = 0, LOBE_SPEC = 1, LOBE_MIRROR = 2, LOBE_CONSTANT = 3 };  // brdf.h BrdfType
+enum MatType : int { MAT_MATTE = 0, MAT_KELEMEN = 1, MAT_COOKTORRANCE = 2, MAT_METAL = 3, MAT_CONSTANT = 4,
+                     MAT_GLASS = 5 };
+// brdf.h BrdfType; LOBE_MIRROR (SpecMirror) and LOBE_TRANSMIT (SpecTransmit) are both the
+// reference's MirrorBrdf: delta lobes without next-event estimation
+enum LobeType : int { LOBE_MATTE = 0, LOBE_SPEC = 1, LOBE_MIRROR = 2, LOBE_CONSTANT = 3, LOBE_TRANSMIT = 4 };
 enum LightType : int { LIGHT_SQUARE = 0, LIGHT_SPHERE = 1 };
 
 struct Material {            // 80 B
@@ -36,7 +39,7 @@ struct Material {            // 80 B
     float refl;              // Kelemen reflectance (selects the albedo table)
     float mix;               // metal mix
     int table;               // Kelemen albedo table index (64x32 floats each)
-    int pad;
+    float ior;               // glass index of refraction
 };
 struct Attr {                // AttributeState: material + emission (attributeState.h)
     int material;
@@ -146,9 +149,17 @@ AUR_HD float3 tex_read(const ShadeScene& s, int tex, float su, float sv) {
 // ------------------------------------------------------------------ BRDF lobes
 struct Brdf {                // an instantiated lobe: BrdfState{Brdf*, bxdfParameters*}
     int lobe;                // LobeType
-    float3 color;            // Lambert albedo or CT colour
-    float rough;             // CT roughness
+    float3 color;            // Lambert albedo, CT colour, mirror / transmission colour
+    float rough;             // CT roughness; LOBE_TRANSMIT: the index of refraction
 };
+
+// worldToTangent (math_utils.h:92-97): components along the UNNORMALISED frame vectors
+// of coordinateSystem (tangentToWorld normalises them), as the reference computes them.
+AUR_HD float3 world_to_tangent(float3 dir, float3 n) {
+    float3 dpdu, dpdv;
+    coordinate_system(n, &dpdu, &dpdv);
+    return mk(dot(dir, dpdu), dot(dir, dpdv), dot(dir, n));
+}
 struct BrdfSample { float3 dir; float pdf; float3 color; float maxt; };
 
 // `albedo * M_PI_INV` with the reference's unparenthesised #define M_PI_INV 1.f/M_PI
@@ -193,6 +204,34 @@ AUR_HD BrdfSample brdf_sample(const Brdf& b, float3 V, float3 N, float r1, float
             if (s.pdf > 100000.f) { s.pdf *= 0.01f; s.color *= 0.01f; }
         }
         s.dir = L;
+        s.maxt = 10000000.f;
+        return s;
+    }
+    if (b.lobe == LOBE_MIRROR) {                                     // specMirror.cpp:35-40
+        const float3 vt = world_to_tangent(V, N);
+        s.dir = normalize(tangent_to_world(mk(-vt.x, -vt.y, vt.z), N));
+        s.pdf = 1.f;
+        s.color = b.color;
+        s.maxt = 100000000.f;
+        return s;
+    }
+    if (b.lobe == LOBE_TRANSMIT) {                                   // specTransmit.cpp:33-56
+        const float costheta = dot(N, V);
+        float ei = 1.f, et = b.rough;
+        if (costheta < 0.f) { ei = b.rough; et = 1.f; }
+        const float sini2 = fmaxf(0.f, 1.f - costheta * costheta);
+        const float eta = ei / et;
+        const float sint2 = eta * eta * sini2;
+        if (sint2 >= 1.f) {   // total internal reflection: Sample3D(Ray(), 0, Color(0)) ends the path
+            s.dir = mk(0.f, 0.f, 0.f); s.pdf = 0.f; s.color = mk(0.f, 0.f, 0.f); s.maxt = 0.f;
+            return s;
+        }
+        float cost = sqrtf(fmaxf(0.f, 1.f - sint2));
+        if (costheta > 0.f) cost = -cost;
+        const float3 vl = world_to_tangent(V, N);
+        s.dir = normalize(tangent_to_world(mk(eta * -vl.x, eta * -vl.y, cost), N));
+        s.pdf = 1.f;
+        s.color = b.color;
         s.maxt = 10000000.f;
         return s;
     }
@@ -294,6 +333,21 @@ AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float 
         b.lobe = LOBE_SPEC;
         b.color = sc * m.gain;
         b.rough = rough;
+        return b;
+    }
+    if (m.type == MAT_GLASS) {                                         // glassMaterial.cpp:33-56
+        b.rough = 0.f;
+        b.lobe = LOBE_MIRROR;
+        b.color = m.spec;
+        if (m.refl == 1.f) return b;
+        float costheta = (float)((double)dot(V, N) * 0.5);            // the reference halves V.N
+        if (costheta < 0.f) costheta = -costheta;
+        const float albedo = schlick(costheta, m.refl);
+        if (lobe_u > albedo) {
+            b.lobe = LOBE_TRANSMIT;
+            b.color = m.diff;                                          // transmitColor
+            b.rough = m.ior;
+        }
         return b;
     }
     b.lobe = LOBE_CONSTANT;

@@ -72,7 +72,7 @@ extern "C" aur_status aur_shading_probe(aur_ctx* ctx, aur_scene* scene, int kind
         return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: cannot read inputs");
     for (uint32_t i = 0; i < n; ++i) {
         const float idx = h[(size_t)i * kInH[kind]];
-        if (kind <= 2 && (idx < 0.f || idx > 3.f)) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: bad lobe");
+        if (kind <= 2 && (idx < 0.f || idx > 4.f)) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: bad lobe");
         if (kind == 3) {
             if (idx < 0.f || idx > 20.f) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: bad table");
             cudaError_t e = ctx_kelemen_ensure(ctx, (int)idx);

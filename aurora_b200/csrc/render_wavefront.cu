@@ -380,7 +380,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 const Frame f = hit_frame(sc.sh, prim, hh.x, hh.y, hh.z, mk(ro.x, ro.y, ro.z), mk(rd.x, rd.y, rd.z), true);
                 const Attr at = sc.sh.attrs[f.attr];
                 if (kind == RAY_DIFFUSE) matte = true;
-                if (kind == RAY_CAMERA) Lo += T * at.emission;
+                if (collects_emission(kind)) Lo += T * at.emission;
                 const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
                                            rng.u(vertex_dim(vtx, kDimLobe)));
                 // next-event estimation: rays and their unoccluded contributions
@@ -443,28 +443,13 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 bool alive = false;
                 const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                                   rng.u(vertex_dim(vtx, kDimBrdf + 1)));
-                if (bs.pdf > 0.f) {
-                    const float cosl = dot(f.N, bs.dir);
-                    T *= cdiv(bs.color * cosl, bs.pdf);
-                    if (bounces > S.p.min_depth) cont *= lum(bs.color) * cosl / bs.pdf;
-                    if (!is_black(T)) {
-                        kind = brdf.lobe == LOBE_SPEC ? RAY_SPECULAR : RAY_DIFFUSE;
-                        bool rr_ok = true;
-                        if (bounces > S.p.min_depth) {
-                            if (rng.u(vertex_dim(vtx, kDimRoulette)) > cont) rr_ok = false;
-                            else T = cdiv(T, cont);
-                        }
-                        if (rr_ok) {
-                            ++bounces;
-                            if (vtx + 1 < S.p.max_depth) {
-                                alive = true;
-                                w.ray_o[slot] = make_float4(f.P.x, f.P.y, f.P.z, kRayBias);
-                                w.ray_d[slot] = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.maxt);
-                                w.tp[slot] = make_float4(T.x, T.y, T.z, cont);
-                                w.id[slot].w = pack_flags(vtx + 1, bounces, kind, matte);
-                            }
-                        }
-                    }
+                if (continue_path(brdf, bs, f.N, S.p.min_depth, rng, vtx, T, cont, kind, bounces) &&
+                    vtx + 1 < S.p.max_depth) {
+                    alive = true;
+                    w.ray_o[slot] = make_float4(f.P.x, f.P.y, f.P.z, kRayBias);
+                    w.ray_d[slot] = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.maxt);
+                    w.tp[slot] = make_float4(T.x, T.y, T.z, cont);
+                    w.id[slot].w = pack_flags(vtx + 1, bounces, kind, matte);
                 }
                 lo = make_float4(Lo.x, Lo.y, Lo.z, lo.w);
                 // a finished path's flags count its recorded vertices (a missed ray's vertex is not recorded)

@@ -64,6 +64,7 @@ static Material make_material(const aur_material_desc& d) {
     m.rough_b = d.roughness_b;
     m.refl = d.reflectance;
     m.mix = d.mix;
+    m.ior = d.ior;
     m.table = d.type == AUR_MAT_KELEMEN ? kelemen_index(d.reflectance) : 0;
     return m;
 }

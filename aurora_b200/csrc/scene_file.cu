@@ -8,7 +8,7 @@
 //   options    resolution, pixelsamples, lightsamples, mindepth, maxdepth, filename
 //   renderCam  fov (slope factor, camera.cpp:51-52), transforms (camera to world)
 //   shaders    texture2DShader (texture files in PFM; EXR needs OpenEXR, not in this build)
-//   materials  matteMaterial, kelemenMaterial, metalMaterial
+//   materials  matteMaterial, kelemenMaterial, metalMaterial, glassMaterial
 //   objects    geometry (OBJ triangles, optional Loop subdivision), light (square)
 //
 // Objects of a JSON object are visited in key order, as the reference's JSON
@@ -908,6 +908,7 @@ struct Loader {
             memset(&m, 0, sizeof(m));
             m.diffuse_tex = m.specular_tex = m.roughness_tex = -1;
             m.gain[0] = m.gain[1] = m.gain[2] = 1.f;
+            m.ior = 1.f;
             if (type == "matteMaterial") {
                 m.type = AUR_MAT_MATTE;
                 color_attr(o, "color", m.diffuse, &m.diffuse_tex, where);
@@ -924,8 +925,12 @@ struct Loader {
                 float_attr(o, "roughnessB", &m.roughness_b, nullptr, where);
                 float_attr(o, "mix", &m.mix, nullptr, where);
                 color_attr(o, "gain", m.gain, nullptr, where);
-            } else if (type == "glassMaterial") {
-                throw_load(AUR_ERR_UNSUPPORTED, where + ": glassMaterial (specular mirror/transmission lobes) is not built");
+            } else if (type == "glassMaterial") {   // constants only, as the reference reads them
+                m.type = AUR_MAT_GLASS;
+                color_attr(o, "specColor", m.specular, nullptr, where);
+                color_attr(o, "transmitColor", m.diffuse, nullptr, where);
+                float_attr(o, "reflectance", &m.reflectance, nullptr, where);
+                float_attr(o, "ior", &m.ior, nullptr, where);
             } else {
                 throw_load(AUR_ERR_PARSE, where + ": unknown material type " + type);
             }
@@ -1079,6 +1084,7 @@ struct Loader {
         black.type = AUR_MAT_CONSTANT;
         black.diffuse_tex = black.specular_tex = black.roughness_tex = -1;
         black.gain[0] = black.gain[1] = black.gain[2] = 1.f;
+        black.ior = 1.f;
         out.materials.push_back(black);
         for (auto& l : lights) {
             out.attr_material.push_back(constant);

@@ -195,9 +195,9 @@ class SceneData:
 
 
 def _mat(type_, diffuse=(0, 0, 0), specular=(0, 0, 0), gain=(1, 1, 1), roughness=0.0, roughness_b=0.0,
-         reflectance=0.0, mix=0.0, diffuse_tex=-1, specular_tex=-1, roughness_tex=-1) -> _abi.MaterialDesc:
+         reflectance=0.0, mix=0.0, diffuse_tex=-1, specular_tex=-1, roughness_tex=-1, ior=1.0) -> _abi.MaterialDesc:
     return _abi.MaterialDesc(type_, _abi.f3(*diffuse), _abi.f3(*specular), _abi.f3(*gain), roughness, roughness_b,
-                             reflectance, mix, diffuse_tex, specular_tex, roughness_tex)
+                             reflectance, mix, diffuse_tex, specular_tex, roughness_tex, ior)
 
 
 def _xform_f32(m: np.ndarray, p: np.ndarray) -> np.ndarray:

@@ -114,7 +114,8 @@ enum {
     AUR_MAT_KELEMEN = 1,
     AUR_MAT_COOKTORRANCE = 2,
     AUR_MAT_METAL = 3,
-    AUR_MAT_CONSTANT = 4
+    AUR_MAT_CONSTANT = 4,
+    AUR_MAT_GLASS = 5      /* glassMaterial: specular mirror / transmission (glassMaterial.cpp:33-56) */
 };
 enum { AUR_LIGHT_SQUARE = 0, AUR_LIGHT_SPHERE = 1 };
 
@@ -130,6 +131,8 @@ typedef struct aur_material_desc {
     int32_t diffuse_tex;   /* texture index or -1 (texture2DShader) */
     int32_t specular_tex;
     int32_t roughness_tex; /* float shader: red channel */
+    float ior;             /* glass index of refraction (glass: specular = specColor,
+                              diffuse = transmitColor, reflectance = Schlick F0, 1 = mirror) */
 } aur_material_desc;
 
 /* Square light: Aurora/src/lights/squareLight.{h,cpp}; the quad
@@ -211,8 +214,8 @@ typedef struct aur_render_opts {
  * (matteMaterial, kelemenMaterial, metalMaterial), objects (geometry: OBJ
  * triangles with optional Loop subdivision, objTriangleMesh.cpp:26-92 and
  * loopSubdivMesh.cpp:167-744; light: square lights). Relative paths resolve
- * against the file's directory. glassMaterial, environment lights, normal maps
- * and triplanar shaders return AUR_ERR_UNSUPPORTED.
+ * against the file's directory. Environment lights, normal maps and triplanar
+ * shaders return AUR_ERR_UNSUPPORTED.
  * aur_scene_file_read flattens the file on the host (no device work) into
  * arrays owned by the aur_scene_file; aur_scene_file_desc points a scene
  * description at them and fills *opts (may be NULL) from "options"

@@ -153,7 +153,7 @@ inline bool triIntersect(const Point& p1, const Vector& e1, const Vector& e2, co
 struct Tri { Point p1; Vector e1, e2; };
 struct Mat {
     int type; Color diff, spec, gain; float rough, roughB, refl, mix;
-    int diffTex, specTex, roughTex; int table;
+    int diffTex, specTex, roughTex; int table; float ior;
 };
 struct Light {
     int type; float xScale, yScale, radius; Point pCam[4]; Vector lightN; Color le; Point center; float m[16];
@@ -388,8 +388,10 @@ static Ray convertSample(const Scene& sc, int x, int y, float j1, float j2) {
 }
 
 // ------------------------------------------------------------ BRDFs
-enum { MatteBrdf = 0, SpecBrdf = 1, MirrorBrdf = 2, ConstantBrdf = 3 };
-struct BrdfState { int type; Color color; float roughness; };
+// MirrorBrdf: SpecMirror; TransmitBrdf: SpecTransmit (the reference's type for both is MirrorBrdf)
+enum { MatteBrdf = 0, SpecBrdf = 1, MirrorBrdf = 2, ConstantBrdf = 3, TransmitBrdf = 4 };
+struct BrdfState { int type; Color color; float roughness; };   // TransmitBrdf: roughness holds the ior
+inline bool isMirrorType(int t) { return t == MirrorBrdf || t == TransmitBrdf; }
 
 static Sample3D lambertGetSample(const BrdfState& b, const Vector& Vn, const Vector& Nn, float r1, float r2) {   // lambert.h:44-62
     Vector dir = SampleHemisphereUniform(r1, r2);
@@ -459,9 +461,50 @@ static Color ctEval(const BrdfState& b, const Vector& Ln, const Vector& Vn, cons
     return b.color * D / (4. * vdoth * vdoth);
 }
 
+static Vector worldToTangent(const Vector& dir, const Vector& Nn) {            // math_utils.h:92-97
+    Vector dPdu, dPdv;
+    coordinateSystem(Nn, &dPdu, &dPdv);
+    return Vector(dot(dir, dPdu), dot(dir, dPdv), dot(dir, Nn));
+}
+static Sample3D mirrorGetSample(const BrdfState& b, const Vector& Vn, const Vector& Nn) {   // specMirror.cpp:35-40
+    Vector Vt = worldToTangent(Vn, Nn);
+    Vector R = Vector(-Vt.x, -Vt.y, Vt.z);
+    R = tangentToWorld(R, Nn);
+    Sample3D s;
+    s.ray.direction = normalize(R); s.ray.origin = Point(0, 0, 0); s.ray.mint = RAY_BIAS; s.ray.maxt = 100000000.f;
+    s.pdf = 1.f; s.color = b.color;
+    return s;
+}
+static Sample3D transmitGetSample(const BrdfState& b, const Vector& Vn, const Vector& Nn) { // specTransmit.cpp:33-56
+    const float ior = b.roughness;
+    float costheta = dot(Nn, Vn);
+    float ei = 1, et = ior;
+    if (costheta < 0.) { ei = ior; et = 1.; }
+    float sini2 = std::max(0.f, 1 - costheta * costheta);
+    float eta = ei / et;
+    float sint2 = eta * eta * sini2;
+    Sample3D s;
+    if (sint2 >= 1.) {
+        s.ray.direction = Vector(0, 0, 0); s.ray.origin = Point(); s.ray.mint = 0; s.ray.maxt = 0;
+        s.pdf = 0.f; s.color = Color(0.f);
+        return s;
+    }
+    float cost = sqrtf(std::max(0.f, 1 - sint2));
+    if (costheta > 0.) cost = -cost;
+    float sintOverSini = eta;
+    Vector Vl = worldToTangent(Vn, Nn);
+    Vector T = Vector(sintOverSini * -Vl.x, sintOverSini * -Vl.y, cost);
+    T = tangentToWorld(T, Nn);
+    s.ray.direction = normalize(T); s.ray.origin = Point(0, 0, 0); s.ray.mint = RAY_BIAS; s.ray.maxt = 10000000.f;
+    s.pdf = 1.f; s.color = b.color;
+    return s;
+}
+
 static Sample3D brdfGetSample(const BrdfState& b, const Vector& V, const Vector& N, float r1, float r2) {
     if (b.type == MatteBrdf) return lambertGetSample(b, V, N, r1, r2);
     if (b.type == SpecBrdf) return ctGetSample(b, V, N, r1, r2);
+    if (b.type == MirrorBrdf) return mirrorGetSample(b, V, N);
+    if (b.type == TransmitBrdf) return transmitGetSample(b, V, N);
     Sample3D s;                                   // Constant::getSample returns Sample3D() (constant.cpp:23-25)
     s.ray.direction = Vector(0, 1, 0); s.ray.origin = Point(); s.ray.mint = 0; s.ray.maxt = 0;
     s.pdf = 0; s.color = Color(0.f);
@@ -545,6 +588,15 @@ static BrdfState getBrdf(const Scene& sc, int matId, const Vector& Vn, const Vec
         float rough = lobeU > m.mix ? m.rough : m.roughB;
         if (mattePath) rough = rough * (1. - CAUSTIC_BLUR) + CAUSTIC_BLUR;
         b.type = SpecBrdf; b.color = sc_ * m.gain; b.roughness = rough;
+        return b;
+    }
+    if (m.type == AUR_MAT_GLASS) {                                   // glassMaterial.cpp:33-56
+        b.type = MirrorBrdf; b.color = m.spec; b.roughness = 0;
+        if (m.refl == 1.f) return b;
+        float costheta = dot(Vn, Nn) * 0.5;
+        if (costheta < 0.f) costheta = -costheta;
+        float albedo = schlick(costheta, m.refl);
+        if (lobeU > albedo) { b.type = TransmitBrdf; b.color = m.diff; b.roughness = m.ior; }
         return b;
     }
     b.type = ConstantBrdf; b.color = Color(0.f); b.roughness = 0;
@@ -770,7 +822,7 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
     return result;
 }
 
-enum { CameraRay = 0, DiffuseRay = 1, SpecularRay = 2 };
+enum { CameraRay = 0, DiffuseRay = 1, SpecularRay = 2, MirrorRay = 3 };
 
 static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng, int maxDepth, int minDepth,
                                    float* alpha, Counts& cnt) {
@@ -790,22 +842,28 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
         LocalGeometry lg = hitGeometry(sc, ray, prim, t, u, v);
         const int vtx = trueBounces;
         if (rayType == DiffuseRay) mattePath = true;
-        if (rayType == CameraRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
+        if (rayType == CameraRay || rayType == MirrorRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
         BrdfState brdf = getBrdf(sc, sc.attrMat[lg.attr], lg.Vn, lg.Nn, lg.su, lg.sv, mattePath, rng(vdim(vtx, DIM_LOBE)));
         Lo += integrateDirect(sc, lg, brdf, rng, vtx, cnt) * pathThroughput;
         Sample3D cur = brdfGetSample(brdf, lg.Vn, lg.Nn, rng(vdim(vtx, DIM_BRDF)), rng(vdim(vtx, DIM_BRDF + 1)));
         if (cur.pdf <= 0.f) break;
-        pathThroughput *= cur.color * dot(lg.Nn, cur.ray.direction) / cur.pdf;
-        if (bounces > minDepth) continueProbability *= cur.color.lum() * dot(lg.Nn, cur.ray.direction) / cur.pdf;
-        if (pathThroughput.isBlack()) break;
-        rayType = brdf.type == SpecBrdf ? SpecularRay : DiffuseRay;
+        if (!isMirrorType(brdf.type)) {
+            pathThroughput *= cur.color * dot(lg.Nn, cur.ray.direction) / cur.pdf;
+            if (bounces > minDepth) continueProbability *= cur.color.lum() * dot(lg.Nn, cur.ray.direction) / cur.pdf;
+            if (pathThroughput.isBlack()) break;
+            rayType = brdf.type == SpecBrdf ? SpecularRay : DiffuseRay;
+        } else {                                                           // integrator.cpp:233-239
+            pathThroughput *= cur.color;
+            if (bounces > minDepth) continueProbability *= cur.color.lum();
+            rayType = MirrorRay;
+        }
         if (bounces > minDepth) {
             if (rng(vdim(vtx, DIM_ROULETTE)) > continueProbability) break;
             pathThroughput /= continueProbability;
         }
         cur.ray.origin = lg.P;
         ++trueBounces;
-        ++bounces;
+        if (!isMirrorType(brdf.type)) ++bounces;
         if (trueBounces >= maxDepth) break;   // unshaded last ray skipped (no environment lights)
         ray = cur.ray;
         ++cnt.closest;
@@ -902,7 +960,7 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         LocalGeometry lg = hitGeometry(sc, ray, prim, t, u, v);
         const int vtx = trueBounces;
         if (rayType == DiffuseRay) mattePath = true;
-        if (rayType == CameraRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
+        if (rayType == CameraRay || rayType == MirrorRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
         const float lobeU = rng(vdim(vtx, DIM_LOBE));
         const int matId = sc.attrMat[lg.attr];
         BrdfState brdf = getBrdf(sc, matId, lg.Vn, lg.Nn, lg.su, lg.sv, mattePath, lobeU);
@@ -928,6 +986,23 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         }
         Sample3D cur = brdfGetSample(brdf, lg.Vn, lg.Nn, rng(vdim(vtx, DIM_BRDF)), rng(vdim(vtx, DIM_BRDF + 1)));
         if (cur.pdf <= 0.f) break;
+        if (isMirrorType(brdf.type)) {     // delta lobe: T *= colour; no parameter of its own
+            for (auto& e : dT) { e.d[0] *= cur.color.r; e.d[1] *= cur.color.g; e.d[2] *= cur.color.b; }
+            pathThroughput *= cur.color;
+            if (bounces > minDepth) continueProbability *= cur.color.lum();
+            rayType = MirrorRay;
+            if (bounces > minDepth) {
+                if (rng(vdim(vtx, DIM_ROULETTE)) > continueProbability) break;
+                pathThroughput /= continueProbability;
+                for (auto& e : dT) for (int c = 0; c < 3; ++c) e.d[c] /= continueProbability;
+            }
+            cur.ray.origin = lg.P;
+            ++trueBounces;
+            if (trueBounces >= maxDepth) break;
+            ray = cur.ray;
+            if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) break;
+            continue;
+        }
         const float cosl = dot(lg.Nn, cur.ray.direction);
         const double w[3] = {(double)cur.color.r * cosl / cur.pdf, (double)cur.color.g * cosl / cur.pdf,
                              (double)cur.color.b * cosl / cur.pdf};
@@ -993,6 +1068,7 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
         mt.gain = Color(md.gain[0], md.gain[1], md.gain[2]);
         mt.rough = md.roughness; mt.roughB = md.roughness_b; mt.refl = md.reflectance; mt.mix = md.mix;
         mt.diffTex = md.diffuse_tex; mt.specTex = md.specular_tex; mt.roughTex = md.roughness_tex;
+        mt.ior = md.ior;
         // KelemenMaterial ctor: modrefl = roundf(reflectance*20)/20 selects the cache (kelemenMaterial.cpp:49-52)
         mt.table = md.type == AUR_MAT_KELEMEN ? std::max(0, std::min(REFL_ENTRIES - 1, (int)roundf(md.reflectance * (REFL_ENTRIES - 1)))) : 0;
         sc->mats.push_back(mt);

@@ -54,6 +54,21 @@ def test_texture_scene(ctx, oracle_lib, kelemen_tables):
     compare(g, mean, m2, 8)
 
 
+GLASS = dict(type_=5, specular=(1.0, 1.0, 1.0), diffuse=(0.95, 0.9, 0.85), reflectance=0.04, ior=1.5)
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_glass_boxes(ctx, oracle_lib, kelemen_tables, mode):
+    """glassMaterial boxes: Fresnel-chosen mirror / transmission lobes, the MirrorRay branch
+    (emission seen through glass, no next-event estimate, no roulette depth), with
+    roulette from the second bounce."""
+    from aurora_b200 import scenes
+    data = scenes.box_scene(128, 128, max_depth=8, box_mat=GLASS)
+    data.render["min_depth"] = 1
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16, mode=mode)
+    compare(g, mean, m2, 16)
+
+
 def test_terrain_small(ctx, oracle_lib, kelemen_tables):
     """The large-scene generator at reduced size (roulette, 16 materials, 4 lights, depth 8)."""
     from aurora_b200 import scenes

@@ -103,3 +103,16 @@ def test_lights_and_materials(ctx, oracle_lib, kelemen_tables):
                            r.uniform(0, 1, (n, 2)), r.integers(0, 2, n)[:, None], r.uniform(0, 1, n)[:, None]],
                           1).astype(np.float32)
     close(ctx.probe(9, mats, scene), osc.probe(9, mats), frac=1e-3)
+
+
+def test_mirror_and_transmission_lobes(ctx, oracle_lib):
+    """Glass lobes (SpecMirror, SpecTransmit): sampled directions, pdf 1, colour."""
+    r = np.random.default_rng(31)
+    n = 4000
+    N = rand_dirs(r, n)
+    V = rand_dirs(r, n)       # both sides of the surface: transmission enters or reflects totally
+    lobe = np.where(r.uniform(size=n) < 0.5, 2, 4)
+    ior = np.where(lobe == 4, r.uniform(1.1, 2.4, n), 0.0)
+    rec = np.concatenate([lobe[:, None], r.uniform(0.1, 1, (n, 3)), ior[:, None], V, N, r.uniform(0, 1, (n, 2))],
+                         1).astype(np.float32)
+    close(ctx.probe(0, rec), oracle_lib.probe(0, rec), atol=2e-7)

@@ -199,3 +199,48 @@ def test_kelemen_table_restatement(oracle_lib):
     assert np.all(t0 >= 0) and np.all(t1 >= t0 - 1e-6)
     # reflectance 1 => F = 1; at normal incidence and low roughness the estimator -> 1
     assert abs(t1[63, 1] - 1.0) < 0.02
+
+
+def _frame(n):
+    """coordinateSystem (math_utils.h:107-129): unnormalised tangents."""
+    n = np.asarray(n, np.float64)
+    if n[0] == 0 and n[1] != 0 and n[2] == 0:
+        v2 = np.cross(n, [1.0, 0, 0])
+    else:
+        v2 = np.cross(n, [0, 1.0, 0])
+    return v2, np.cross(n, v2)
+
+
+def test_mirror_and_transmission_known_answers(oracle_lib):
+    """SpecMirror / SpecTransmit (specMirror.cpp:35-40, specTransmit.cpp:33-56) in float64:
+    tangent components taken along the UNNORMALISED frame (worldToTangent) and mapped back
+    along the normalised one (tangentToWorld) — an exact reflection only where the frame is
+    unit length, a scaled one elsewhere, as the reference computes it."""
+    r = np.random.default_rng(12)
+    recs, want = [], []
+    for k in range(200):
+        n = r.normal(size=3); n /= np.linalg.norm(n)
+        v = r.normal(size=3); v /= np.linalg.norm(v)
+        while v @ n < 0.05:
+            v = r.normal(size=3); v /= np.linalg.norm(v)
+        lobe, ior = (2, 0.0) if k % 2 == 0 else (4, 1.5)
+        du, dv = _frame(n)
+        vt = np.array([v @ du, v @ dv, v @ n])
+        if lobe == 2:
+            t = np.array([-vt[0], -vt[1], vt[2]])
+        else:
+            eta = 1 / ior
+            cost = -np.sqrt(max(0.0, 1 - eta * eta * (1 - (v @ n) ** 2)))
+            t = np.array([eta * -vt[0], eta * -vt[1], cost])
+        d = t[0] * du / np.linalg.norm(du) + t[1] * dv / np.linalg.norm(dv) + t[2] * n
+        want.append(d / np.linalg.norm(d))
+        recs.append([lobe, 0.9, 0.8, 0.7, ior, *v, *n, 0.5, 0.5])
+    out = oracle_lib.probe(0, np.array(recs, np.float32))
+    np.testing.assert_allclose(out[:, :3], np.array(want), atol=2e-6)
+    assert np.all(out[:, 3] == 1.0) and np.allclose(out[:, 4:7], [0.9, 0.8, 0.7])
+    # V below the surface: ei = ior, et = 1 and a grazing angle reflects totally (pdf 0)
+    tir = oracle_lib.probe(0, np.array([[4, 1, 1, 1, 1.5, 0.99, 0, -0.141, 0, 0, 1, 0.5, 0.5]], np.float32))
+    assert tir[0, 3] == 0.0 and np.all(tir[0, 4:7] == 0.0)
+    # an exact mirror where the frame is unit length (N orthogonal to y)
+    m = oracle_lib.probe(0, np.array([[2, 1, 1, 1, 0, 0.6, 0, 0.8, 0, 0, 1, 0.5, 0.5]], np.float32))
+    np.testing.assert_allclose(m[0, :3], [-0.6, 0, 0.8], atol=1e-7)

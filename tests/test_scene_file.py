@@ -249,7 +249,9 @@ def test_texture_shader_and_kelemen_material(tmp_path):
 
 @pytest.mark.parametrize("mutate,status", [
     (lambda s: s.pop("options"), _abi.ERR_PARSE),
-    (lambda s: s["materials"].update({"m": {"type": "glassMaterial"}}), _abi.ERR_UNSUPPORTED),
+    (lambda s: s["materials"].update({"m": {"type": "glassMaterial"}}), _abi.ERR_PARSE),
+    (lambda s: s["materials"].update({"m": {"type": "matteMaterial", "color": [1, 1, 1], "normalmap": "n"}}),
+     _abi.ERR_UNSUPPORTED),
     (lambda s: s["objects"].update({"e": {"type": "envlight"}}), _abi.ERR_UNSUPPORTED),
     (lambda s: s["objects"]["g"].update({"material": "nope"}), _abi.ERR_PARSE),
     (lambda s: s["objects"]["g"].update({"path": "missing.obj"}), _abi.ERR_IO),
@@ -284,3 +286,14 @@ def test_exr_textures_are_refused(tmp_path):
     with pytest.raises(_abi.AuroraError) as e:
         scenes.load_scene_file(write_single(str(tmp_path), "q.obj", 0, materials=mats, shaders=shaders))
     assert e.value.status == _abi.ERR_UNSUPPORTED and "OpenEXR" in str(e.value)
+
+
+def test_glass_material(tmp_path):
+    v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
+    write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
+    mats = {"m": {"type": "glassMaterial", "specColor": [1, 1, 1], "transmitColor": [0.9, 0.8, 0.7],
+                  "reflectance": 0.04, "ior": 1.5}}
+    data, _, _ = scenes.load_scene_file(write_single(str(tmp_path), "q.obj", 0, materials=mats))
+    m = data.materials[0]
+    assert m.type == _abi.MAT_GLASS and m.ior == np.float32(1.5) and m.reflectance == np.float32(0.04)
+    assert tuple(m.specular) == (1, 1, 1) and np.allclose(tuple(m.diffuse), (0.9, 0.8, 0.7))
