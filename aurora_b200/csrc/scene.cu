@@ -144,8 +144,10 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     std::vector<Material> mats(d->nmat);
     for (uint32_t m = 0; m < d->nmat; ++m) {
         const aur_material_desc& md = d->materials[m];
-        if (md.type < AUR_MAT_MATTE || md.type > AUR_MAT_CONSTANT)
+        if (md.type < AUR_MAT_MATTE || md.type > AUR_MAT_GLASS)
             return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: unknown material type");
+        if (md.type == AUR_MAT_GLASS && !(md.ior > 0.f))
+            return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: glass needs an index of refraction > 0");
         const int tx[3] = {md.diffuse_tex, md.specular_tex, md.roughness_tex};
         for (int k = 0; k < 3; ++k)
             if (tx[k] >= (int)d->ntex || tx[k] < -1) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: texture index");

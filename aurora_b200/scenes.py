@@ -364,11 +364,13 @@ FOV40 = math.tan(math.radians(20.0))
 
 # ----------------------------------------------------------------------------- workloads
 def box_scene(width=256, height=256, spp=16, max_depth=5, seed=1, rng_seed=None, wall=(0.73, 0.73, 0.73),
-              red=(0.65, 0.05, 0.05), green=(0.12, 0.45, 0.15), box_mat=None) -> SceneData:
+              red=(0.65, 0.05, 0.05), green=(0.12, 0.45, 0.15), box_mat=None, lift=0.0) -> SceneData:
     """Closed box: 5 wall quads of side 2 (10 tris), two rotated boxes (24 tris), a 0.5x0.5 ceiling
     light of radiance (17,12,4); Lambert walls, Cook-Torrance boxes (roughness 0.3, F0 0.04);
     40 degree pinhole; roulette off (min_depth = max_depth). With `rng_seed` the box poses and
-    materials are drawn from that seed (the 64-scene batch)."""
+    materials are drawn from that seed (the 64-scene batch). `lift` raises the boxes off the floor
+    (their bottom faces otherwise lie in the floor's plane, where rays inside a transparent box
+    hit both at exactly the same distance)."""
     b = SceneBuilder(width, height, FOV40, world_to_camera=translate(0, 0, -3.5), name="box")
     r = np.random.default_rng(rng_seed) if rng_seed is not None else None
     if r is not None:
@@ -401,7 +403,7 @@ def box_scene(width=256, height=256, spp=16, max_depth=5, seed=1, rng_seed=None,
             x = (0.4 if k else -0.35) + float(r.uniform(-0.15, 0.15))
             poses.append((x, -1 + h / 2, float(r.uniform(-0.5, 0.4)), 0.55, h, 0.55, float(r.uniform(-40, 40))))
     for (x, y, z, sx, sy, sz, ry) in poses:
-        o2w = translate(x, y, z) @ rot_y(ry) @ scale(sx, sy, sz)
+        o2w = translate(x, y + lift, z) @ rot_y(ry) @ scale(sx, sy, sz)
         b.mesh(bv, bf, m_box, normals=None, object_to_world=o2w)
     b.square_light(translate(0, 0.999, 0) @ rot_x(-90.0), 0.25, 0.25, (17.0, 12.0, 4.0), 0.0)
     return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))

@@ -960,7 +960,20 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         LocalGeometry lg = hitGeometry(sc, ray, prim, t, u, v);
         const int vtx = trueBounces;
         if (rayType == DiffuseRay) mattePath = true;
-        if (rayType == CameraRay || rayType == MirrorRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
+        if (rayType == CameraRay || rayType == MirrorRay) {
+            const Color& E = sc.attrEmission[lg.attr];
+            Lo += pathThroughput * E;
+            // emission seen through mirror / transmission vertices carries dT
+            for (const auto& e : dT) {
+                if (e.perChannel) {
+                    contrib.push_back({e.base + 0, delta[0] * e.d[0] * E.r});
+                    contrib.push_back({e.base + 1, delta[1] * e.d[1] * E.g});
+                    contrib.push_back({e.base + 2, delta[2] * e.d[2] * E.b});
+                } else {
+                    contrib.push_back({e.base, delta[0] * e.d[0] * E.r + delta[1] * e.d[1] * E.g + delta[2] * e.d[2] * E.b});
+                }
+            }
+        }
         const float lobeU = rng(vdim(vtx, DIM_LOBE));
         const int matId = sc.attrMat[lg.attr];
         BrdfState brdf = getBrdf(sc, matId, lg.Vn, lg.Nn, lg.su, lg.sv, mattePath, lobeU);

@@ -68,7 +68,7 @@ def test_adjoint_matches_fp64_oracle_through_glass(ctx, kelemen_tables, oracle_l
     from aurora_b200 import _abi, scenes
     glass = dict(type_=_abi.MAT_GLASS, specular=(1.0, 1.0, 1.0), diffuse=(0.95, 0.9, 0.85), reflectance=0.04,
                  ior=1.5)
-    data = scenes.box_scene(128, 128, spp=64, max_depth=8, box_mat=glass)
+    data = scenes.box_scene(128, 128, spp=64, max_depth=8, box_mat=glass, lift=0.01)
     data.render["min_depth"] = 1
     gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (40, 72, 32, 32), 64, 1, 23, mode)
     assert np.count_nonzero(cm[:3, :3]) == 9

@@ -63,7 +63,7 @@ def test_glass_boxes(ctx, oracle_lib, kelemen_tables, mode):
     (emission seen through glass, no next-event estimate, no roulette depth), with
     roulette from the second bounce."""
     from aurora_b200 import scenes
-    data = scenes.box_scene(128, 128, max_depth=8, box_mat=GLASS)
+    data = scenes.box_scene(128, 128, max_depth=8, box_mat=GLASS, lift=0.01)
     data.render["min_depth"] = 1
     g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16, mode=mode)
     compare(g, mean, m2, 16)

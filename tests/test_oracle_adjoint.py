@@ -74,3 +74,22 @@ def test_oracle_adjoint_texel_matches_fd(oracle_lib):
     assert abs(gt[i] - fd) <= 0.01 * abs(fd) + 1e-6, (i, gt[i], fd)
     # the textured ground owns no constant diffuse gradient
     assert np.all(gm[0, :3] == 0.0)
+
+
+def test_oracle_adjoint_through_glass_matches_fd(oracle_lib):
+    """Glass boxes (mirror and transmission vertices, emission seen through them): the
+    wall albedo gradients against central differences, roulette off."""
+    from aurora_b200 import _abi, scenes
+    glass = dict(type_=_abi.MAT_GLASS, specular=(1.0, 1.0, 1.0), diffuse=(0.95, 0.9, 0.85), reflectance=0.04,
+                 ior=1.5)
+    data = scenes.box_scene(64, 64, spp=8, max_depth=6, box_mat=glass, lift=0.01)
+    tables = np.zeros((21, 64, 32), np.float32)
+    w = np.random.default_rng(9).normal(size=(64, 64, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    crop, spp, seed = (16, 24, 32, 32), 8, 1
+    gm, _ = oracle_lib.OracleScene(data, tables).adjoint(spp, 6, 6, seed, w, crop=crop)
+    h = 1e-2
+    for m, c in [(0, 1), (1, 0), (2, 2)]:
+        fd = (_loss(oracle_lib, _perturbed_material(data, m, c, h), tables, w, spp, crop, seed) -
+              _loss(oracle_lib, _perturbed_material(data, m, c, -h), tables, w, spp, crop, seed)) / (2 * h)
+        assert abs(gm[m, c] - fd) <= 0.01 * abs(fd) + 1e-6, (m, c, gm[m, c], fd)
