@@ -26,7 +26,7 @@ STATUS_NAMES = {0: "AUR_OK", 1: "AUR_ERR_INVALID_ARG", 2: "AUR_ERR_OOM", 3: "AUR
                 5: "AUR_ERR_QUEUE_OVERFLOW", 6: "AUR_ERR_PARSE", 7: "AUR_ERR_IO", 8: "AUR_ERR_UNSUPPORTED"}
 
 MAT_MATTE, MAT_KELEMEN, MAT_COOKTORRANCE, MAT_METAL, MAT_CONSTANT, MAT_GLASS = 0, 1, 2, 3, 4, 5
-LIGHT_SQUARE, LIGHT_SPHERE = 0, 1
+LIGHT_SQUARE, LIGHT_SPHERE, LIGHT_ENV = 0, 1, 2
 ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_QUEUE_OVERFLOW, ERR_PARSE, ERR_IO, ERR_UNSUPPORTED = range(1, 9)
 FILM_PFM, FILM_EXR_HALF, FILM_EXR_FLOAT = 0, 1, 2
 RENDER_PLAIN, RENDER_WAVEFRONT = 0, 1
@@ -56,7 +56,8 @@ class MaterialDesc(C.Structure):
 
 class LightDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("object_to_camera", C.c_float * 16), ("size_x", C.c_float),
-                ("size_y", C.c_float), ("center", f3), ("radius", C.c_float), ("color", f3), ("exposure", C.c_float)]
+                ("size_y", C.c_float), ("center", f3), ("radius", C.c_float), ("color", f3), ("exposure", C.c_float),
+                ("tex", C.c_int32)]
 
 
 class SceneDesc(C.Structure):

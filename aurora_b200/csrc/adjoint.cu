@@ -153,7 +153,7 @@ __device__ __forceinline__ float3 direct(const DevScene& sc, const Frame& f, con
     const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
     if (li < 0) return res;
     const Light L = sc.sh.lights[li];
-    const LightSample ls = light_sample(L, f.P, rng.u(vertex_dim(vtx, kDimLightSample)),
+    const LightSample ls = light_sample(sc.sh, L, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightSample)),
                                         rng.u(vertex_dim(vtx, kDimLightSample + 1)));
     float cost = dot(f.N, ls.dir);
     if (brdf.lobe == LOBE_MATTE) {
@@ -189,14 +189,14 @@ __device__ __forceinline__ float3 direct(const DevScene& sc, const Frame& f, con
         cost = dot(f.N, bs.dir);
         if (cost > 0.f) {
             float maxt = bs.maxt;
-            const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
+            const float lp = light_pdf(sc.sh, L, f.P, bs.dir, kRayBias, &maxt);
             if (lp > 0.f && bs.pdf > 0.f) {
                 bool open;
                 if (kTrace) { ++rc.shadow; open = !bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.shadow_work); if (open) *vis |= 2u; }
                 else open = (*vis & 2u) != 0;
                 if (open) {
                     const float w = power_heuristic(bs.pdf, lp);
-                    const float3 c1 = cdiv(((bs.color * w) * L.le) * cost, bs.pdf);
+                    const float3 c1 = cdiv(((bs.color * w) * light_eval(sc.sh, L, bs.dir)) * cost, bs.pdf);
                     res += c1;
                     if (kGrad) dres += c1 * sample_dlnD(brdf, f, bs);
                 }
@@ -394,6 +394,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
             float3 Lo = mk(0.f, 0.f, 0.f);
             {
                 RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+                const float3 cam_d = ray.d;
                 Hit h;
                 ++rc.closest;
                 if (bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
@@ -418,7 +419,10 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         if (vtx + 1 >= p.max_depth) break;
                         ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
                         ++rc.closest;
-                        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) break;
+                        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+                            if (kind == RAY_MIRROR && sc.sh.nenv) Lo += env_radiance(sc.sh, cam_d) * T;
+                            break;
+                        }
                     }
                 }
             }

@@ -82,6 +82,7 @@ AUR_HD float xtanf(float x) { return (float)tan((double)x); }
 AUR_HD float xatanf(float x) { return (float)atan((double)x); }
 AUR_HD float xcosf(float x) { return (float)cos((double)x); }
 AUR_HD float xsinf(float x) { return (float)sin((double)x); }
+AUR_HD float xatan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
 
 // ---------------------------------------------------------------- float3 helpers
 AUR_HD float3 mk(float x, float y, float z) { float3 r; r.x = x; r.y = y; r.z = z; return r; }

@@ -57,7 +57,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
     const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
     if (li < 0) return res;
     const Light L = sc.sh.lights[li];
-    const LightSample ls = light_sample(L, f.P, rng.u(vertex_dim(vtx, kDimLightSample)),
+    const LightSample ls = light_sample(sc.sh, L, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightSample)),
                                         rng.u(vertex_dim(vtx, kDimLightSample + 1)));
     float cost = dot(f.N, ls.dir);
     if (brdf.lobe == LOBE_MATTE) {
@@ -82,12 +82,12 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
         cost = dot(f.N, bs.dir);
         if (cost > 0.f) {
             float maxt = bs.maxt;
-            const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
+            const float lp = light_pdf(sc.sh, L, f.P, bs.dir, kRayBias, &maxt);
             if (lp > 0.f && bs.pdf > 0.f) {
                 ++rc.shadow;
                 if (!bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.shadow_work)) {
                     const float w = power_heuristic(bs.pdf, lp);
-                    res += cdiv(((bs.color * w) * L.le) * cost, bs.pdf);
+                    res += cdiv(((bs.color * w) * light_eval(sc.sh, L, bs.dir)) * cost, bs.pdf);
                 }
             }
         }
@@ -146,7 +146,12 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
     ++rc.closest;
     *alpha = 0.f;
     float3 Lo = mk(0.f, 0.f, 0.f);
-    if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) return Lo;
+    const float3 cam_d = ray.d;
+    if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+        if (sc.sh.nenv == 0) return Lo;
+        *alpha = 1.f;                       // environment seen directly: not firefly-filtered
+        return env_radiance(sc.sh, cam_d);
+    }
     *alpha = 1.f;
     float3 T = mk(1.f, 1.f, 1.f);
     float cont = 1.f;
@@ -170,7 +175,12 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         ray.mint = kRayBias;
         ray.maxt = bs.maxt;
         ++rc.closest;
-        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) break;
+        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+            // a mirror ray that escapes sees the environment along the CAMERA ray's
+            // direction, as integrator.cpp:262-274 evaluates it
+            if (kind == RAY_MIRROR && sc.sh.nenv) Lo += env_radiance(sc.sh, cam_d) * T;
+            break;
+        }
     }
     return firefly_clamp(Lo);
 }

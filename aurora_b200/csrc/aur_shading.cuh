@@ -27,7 +27,7 @@ enum MatType : int { MAT_MATTE = 0, MAT_KELEMEN = 1, MAT_COOKTORRANCE = 2, MAT_M
 // brdf.h BrdfType; LOBE_MIRROR (SpecMirror) and LOBE_TRANSMIT (SpecTransmit) are both the
 // reference's MirrorBrdf: delta lobes without next-event estimation
 enum LobeType : int { LOBE_MATTE = 0, LOBE_SPEC = 1, LOBE_MIRROR = 2, LOBE_CONSTANT = 3, LOBE_TRANSMIT = 4 };
-enum LightType : int { LIGHT_SQUARE = 0, LIGHT_SPHERE = 1 };
+enum LightType : int { LIGHT_SQUARE = 0, LIGHT_SPHERE = 1, LIGHT_ENV = 2 };
 
 struct Material {            // 80 B
     int type;
@@ -52,7 +52,12 @@ struct Light {
     float3 n;                // lightN = normalize(cross(p1-p2, p2-p3))
     float3 le;               // colour * 2^exposure
     float3 center;           // sphere centre (camera space)
-    float m[16];             // object-to-camera, row major (the square's sample mapping)
+    float m[16];             // square: object-to-camera, row major; env: camera-to-world
+    float minv[16];          // env: world-to-camera (the FP32 Gauss-Jordan inverse of m)
+    int tex;                 // env: env-map texture index, -1 for a constant colour
+    float escale;            // env: 2^exposure (the map's texels are scaled by it)
+    float pdf_norm;          // env: mean texel luminance (Texture2D::initPdf)
+    int pad;
 };
 struct Texture { int w, h, offset, pad; };   // texels: RGB float, offset in floats
 struct Camera { float fov; int w, h; int pad; };
@@ -64,6 +69,7 @@ struct ShadeScene {          // device pointers for the shading stage
     const Texture* texs;
     const float* texels;
     const float* albedo;     // Kelemen tables, [table][cos 64][rough 32]
+    int nenv;                // environment lights among the lights
     const float* corner_n;   // per-corner normals, 9 floats per triangle
     const float* corner_uv;  // per-corner uvs, 6 floats per triangle
     const int* tri_attr;     // attribute index per triangle
@@ -359,7 +365,58 @@ AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float 
 // ------------------------------------------------------------------ lights
 struct LightSample { float3 dir; float maxt; float pdf; float3 color; };
 
+// ---- environment light (InfiniteAreaLight, geometry/infiniteAreaLight.cpp:35-106)
+AUR_HD float3 xform_vector(const float* m, float3 v) {                  // transform.cpp:222-228
+    return mk(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
+              m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+// Texture2D::read / ::pdf with filter 0 at (s, t) (texture2D.cpp:48-72, 112-134): the texel
+// floor(s w), floor(t h), no wrap and no flip (unlike the uv shader lookup)
+AUR_HD int env_texel_index(const Texture& t, float s, float v) {
+    int x = (int)floorf(s * (float)t.w), y = (int)floorf(v * (float)t.h);
+    if (y == t.h) y -= 1;
+    if (x == t.w) x -= 1;
+    x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
+    y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
+    return y * t.w + x;
+}
+AUR_HD float3 env_texel(const ShadeScene& sh, int tex, float s, float v) {
+    const Texture t = sh.texs[tex];
+    const float* p = sh.texels + t.offset + 3 * env_texel_index(t, s, v);
+    return mk(p[0], p[1], p[2]);
+}
+// the map's pdf: texel luminance (r + g + b) / 3 over its mean (Texture2D::initPdf)
+AUR_HD float env_texel_pdf(const ShadeScene& sh, const Light& l, float s, float v) {
+    const float3 c = env_texel(sh, l.tex, s, v);
+    return ((c.x + c.y + c.z) / 3.f) / l.pdf_norm;
+}
+// map coordinates of a camera-space direction (InfiniteAreaLight::eval / ::pdf)
+AUR_HD void env_uv(const Light& l, float3 dir_cam, float* u, float* v) {
+    const float3 dir = xform_vector(l.m, dir_cam);
+    *v = (float)(0.5 * (double)(1.f - dir.y));
+    float uu = (float)((double)xatan2f(dir.z, dir.x) / 6.283185307179586);   // / (M_PI * 2.f) in double
+    if (uu < 0.f) uu += 1.f;
+    *u = uu;
+}
+// radiance arriving along camera-space direction `dir` from a light (Light::eval): the
+// square and sphere lights are constant, the environment reads its map
+AUR_HD float3 light_eval(const ShadeScene& sh, const Light& l, float3 dir) {
+    if (l.type != LIGHT_ENV || l.tex < 0) return l.le;
+    float u, v;
+    env_uv(l, dir, &u, &v);
+    return env_texel(sh, l.tex, u, v) * l.escale;
+}
+// every environment light's radiance along `dir` (camera-ray and mirror-ray misses,
+// integrator.cpp:262-288)
+AUR_HD float3 env_radiance(const ShadeScene& sh, float3 dir) {
+    float3 r = mk(0.f, 0.f, 0.f);
+    for (int i = 0; i < sh.nlights; ++i)
+        if (sh.lights[i].type == LIGHT_ENV) r += light_eval(sh, sh.lights[i], dir);
+    return r;
+}
+
 AUR_HD bool light_visible(const Light& l, float3 P, float3 N) {       // squareLight.h:99-110
+    if (l.type == LIGHT_ENV) return true;
     if (l.type == LIGHT_SQUARE) {
         for (int i = 0; i < 4; ++i)
             if (dot(l.p[i] - P, N) > 0.f) return true;
@@ -397,8 +454,27 @@ AUR_HD float sphere_cone_cos(const Light& l, float3 P) {
     return sqrtf(fmaxf(0.f, 1.f - s2));
 }
 
-AUR_HD LightSample light_sample(const Light& l, float3 P, float u1, float u2) {
+AUR_HD LightSample light_sample(const ShadeScene& sh, const Light& l, float3 P, float3 N, float u1, float u2) {
     LightSample s;
+    if (l.type == LIGHT_ENV) {                                           // infiniteAreaLight.cpp:35-61
+        float3 dirw;
+        float pdf;
+        if (l.tex >= 0) {   // a uniform direction on the sphere, weighted by the map's pdf at (u1, u2)
+            const float vy = 1.f - 2.f * u2;
+            const float r = sqrtf(fmaxf(0.f, 1.f - vy * vy));
+            const float phi = two_pi_times(u1);
+            dirw = xform_vector(l.minv, mk(r * xcosf(phi), vy, r * xsinf(phi)));
+            pdf = env_texel_pdf(sh, l, u1, u2);
+        } else {
+            pdf = 2.f;
+            dirw = tangent_to_world(sample_hemisphere_uniform(u1, u2), N);
+        }
+        s.dir = normalize(dirw);
+        s.maxt = 1000000.f;
+        s.pdf = (float)((double)pdf / 12.566370614359172);               // pdf / (M_PI * 4.)
+        s.color = light_eval(sh, l, s.dir);
+        return s;
+    }
     if (l.type == LIGHT_SQUARE) {                                        // squareLight.h:57-82
         float3 lp = mk((float)(((double)u1 - 0.5) * l.xs * 2.0), (float)(((double)u2 - 0.5) * l.ys * 2.0), 0.f);
         lp = xform_point(l.m, lp);
@@ -434,7 +510,13 @@ AUR_HD LightSample light_sample(const Light& l, float3 P, float u1, float u2) {
 
 // SquareLight::pdf (squareLight.h:88-97): hits the two light triangles, shortens
 // the ray to the light and returns the solid-angle pdf (two-sided, as in the reference).
-AUR_HD float light_pdf(const Light& l, float3 o, float3 d, float mint, float* maxt) {
+AUR_HD float light_pdf(const ShadeScene& sh, const Light& l, float3 o, float3 d, float mint, float* maxt) {
+    if (l.type == LIGHT_ENV) {                                           // infiniteAreaLight.cpp:82-106, hemisphere
+        if (l.tex < 0) return (float)(1.0 / 6.283185307179586);         // 1.f / (M_PI * 2.f)
+        float u, v;
+        env_uv(l, d, &u, &v);
+        return (float)((double)env_texel_pdf(sh, l, u, v) / 6.283185307179586);
+    }
     if (l.type == LIGHT_SQUARE) {
         float t, b1, b2;
         bool hit = tri_intersect(l.p[0], xsub(l.p[1], l.p[0]), xsub(l.p[3], l.p[0]), o, d, mint, *maxt, &t, &b1, &b2);

@@ -8,9 +8,9 @@ using namespace aur;
 
 namespace {
 
-constexpr int kInH[10] = {13, 14, 14, 3, 7, 2, 6, 9, 7, 11};
+constexpr int kInH[10] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11};
 constexpr int kOutH[10] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5};
-__constant__ int kIn[10] = {13, 14, 14, 3, 7, 2, 6, 9, 7, 11};
+__constant__ int kIn[10] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11};
 __constant__ int kOut[10] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5};
 
 __global__ void k_probe(int kind, const float* in, uint32_t n, float* out, ShadeScene sh, const float* tables) {
@@ -41,12 +41,12 @@ __global__ void k_probe(int kind, const float* in, uint32_t n, float* out, Shade
     } else if (kind == 5) {
         o[0] = power_heuristic(q[0], q[1]);
     } else if (kind == 6) {
-        LightSample s = light_sample(sh.lights[(int)q[0]], mk(q[1], q[2], q[3]), q[4], q[5]);
+        LightSample s = light_sample(sh, sh.lights[(int)q[0]], mk(q[1], q[2], q[3]), mk(q[6], q[7], q[8]), q[4], q[5]);
         o[0] = s.dir.x; o[1] = s.dir.y; o[2] = s.dir.z; o[3] = s.maxt; o[4] = s.pdf;
         o[5] = s.color.x; o[6] = s.color.y; o[7] = s.color.z;
     } else if (kind == 7) {
         float maxt = q[8];
-        o[0] = light_pdf(sh.lights[(int)q[0]], mk(q[1], q[2], q[3]), mk(q[4], q[5], q[6]), q[7], &maxt);
+        o[0] = light_pdf(sh, sh.lights[(int)q[0]], mk(q[1], q[2], q[3]), mk(q[4], q[5], q[6]), q[7], &maxt);
         o[1] = maxt;
     } else if (kind == 8) {
         o[0] = light_visible(sh.lights[(int)q[0]], mk(q[1], q[2], q[3]), mk(q[4], q[5], q[6])) ? 1.f : 0.f;

@@ -72,7 +72,9 @@ struct WfPool {
     uint32_t P;
 };
 
-// flags in id.w
+// flags in id.w; kNoClamp: the sample is the environment seen by the camera ray, which
+// the reference adds without the firefly filter
+constexpr uint32_t kNoClamp = 1u << 21;
 __device__ __forceinline__ uint32_t pack_flags(int vtx, int bounces, int kind, bool matte) {
     return (uint32_t)vtx | ((uint32_t)bounces << 9) | ((uint32_t)kind << 18) | ((uint32_t)matte << 20);
 }
@@ -157,7 +159,7 @@ __global__ void k_regen(WfPool w, int in_q) {
             if (kRec) {
                 S.lo_raw[(size_t)id.z * S.npix + id.y] = make_float4(lo.x, lo.y, lo.z, __int_as_float(f_vtx(id.w)));
             } else {
-                const float3 L = firefly_clamp(mk(lo.x, lo.y, lo.z));
+                const float3 L = (id.w & kNoClamp) ? mk(lo.x, lo.y, lo.z) : firefly_clamp(mk(lo.x, lo.y, lo.z));
                 S.samples[(size_t)id.z * S.npix + id.y] = make_float4(L.x, L.y, L.z, lo.w);
             }
             st = PS_EMPTY;
@@ -357,6 +359,27 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
             const int prim = __float_as_int(hh.w);
             float4 lo = w.lo[slot];
             if (prim < 0) {
+                const uint4 id = w.id[slot];
+                const WfScene& S = w.scenes[id.x];
+                const int kind = f_kind(id.w), vtx = f_vtx(id.w);
+                if (S.sc.sh.nenv && (vtx == 0 || kind == RAY_MIRROR)) {
+                    // the environment along the camera ray (integrator.cpp:262-288)
+                    PathRng rng;
+                    rng.key = S.key;
+                    rng.base = path_base(id.y, (uint32_t)S.p.sample_offset + id.z);
+                    const RayF cr = camera_ray(S.sc.cam, (int)(id.y % (uint32_t)S.sc.cam.w),
+                                               (int)(id.y / (uint32_t)S.sc.cam.w), rng.u(kDimCamera),
+                                               rng.u(kDimCamera + 1));
+                    const float3 e = env_radiance(S.sc.sh, cr.d);
+                    if (vtx == 0) {
+                        lo = make_float4(e.x, e.y, e.z, 1.f);
+                        w.id[slot].w = id.w | kNoClamp;
+                    } else {
+                        const float4 t = w.tp[slot];
+                        const float3 a = e * mk(t.x, t.y, t.z);
+                        lo.x += a.x; lo.y += a.y; lo.z += a.z;
+                    }
+                }
                 w.state[slot] = PS_DONE;
             } else {
                 const uint4 id = w.id[slot];
@@ -390,7 +413,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                     const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
                     if (li >= 0) {
                         const Light L = sc.sh.lights[li];
-                        const LightSample ls = light_sample(L, f.P, rng.u(vertex_dim(vtx, kDimLightSample)),
+                        const LightSample ls = light_sample(sc.sh, L, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightSample)),
                                                             rng.u(vertex_dim(vtx, kDimLightSample + 1)));
                         float cost = dot(f.N, ls.dir);
                         float3 c0 = mk(0.f, 0.f, 0.f), c1 = c0;
@@ -416,13 +439,13 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                             cost = dot(f.N, bs.dir);
                             if (cost > 0.f) {
                                 float maxt = bs.maxt;
-                                const float lp = light_pdf(L, f.P, bs.dir, kRayBias, &maxt);
+                                const float lp = light_pdf(sc.sh, L, f.P, bs.dir, kRayBias, &maxt);
                                 if (lp > 0.f && bs.pdf > 0.f) {
                                     r1 = true;
                                     d1 = bs.dir;
                                     m1 = maxt;
                                     const float wgt = power_heuristic(bs.pdf, lp);
-                                    c1 = cdiv(((bs.color * wgt) * L.le) * cost, bs.pdf);
+                                    c1 = cdiv(((bs.color * wgt) * light_eval(sc.sh, L, bs.dir)) * cost, bs.pdf);
                                 }
                             }
                         }

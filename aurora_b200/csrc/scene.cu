@@ -5,6 +5,7 @@
 // objects then light shapes, per-corner normals/uvs (EmbreeMesh, embreeMesh.h:30-63),
 // AttributeState {material, emission} per object/light, materials, lights.
 #include "aur_capi_internal.h"
+#include "aur_host_math.h"
 #include <cmath>
 #include <cstring>
 
@@ -27,14 +28,34 @@ aur_status bvh_options(const aur_bvh_opts* o, BvhBuildOptions* out) {
     return AUR_OK;
 }
 
-// Square light set-up of SquareLight's constructor (squareLight.cpp:20-52).
-static Light make_light(const aur_light_desc& d) {
+// Square light set-up of SquareLight's constructor (squareLight.cpp:20-52); the
+// environment light's (infiniteAreaLight.cpp:21-33, Texture2D::initPdf).
+static Light make_light(const aur_light_desc& d, const std::vector<Texture>& texs, const float* texels) {
     Light l;
     memset(&l, 0, sizeof(l));
     l.type = d.type;
+    l.tex = -1;
     const float inten = powf(2.f, d.exposure);
     l.le = mk(d.color[0] * inten, d.color[1] * inten, d.color[2] * inten);
     for (int k = 0; k < 16; ++k) l.m[k] = d.object_to_camera[k];
+    if (d.type == AUR_LIGHT_ENV) {
+        const float e = (float)pow(2.0, (double)d.exposure);             // pow(2, m_exposure) in eval
+        l.le = mk(d.color[0] * e, d.color[1] * e, d.color[2] * e);
+        l.escale = e;
+        invert4_gj(l.m, l.minv);
+        if (d.tex >= 0) {   // the pdf normalisation: the FP32 running sum of (r + g + b) / 3 over the map
+            l.tex = d.tex;
+            const Texture& t = texs[d.tex];
+            float sum = 0.f;
+            for (int y = 0; y < t.h; ++y)
+                for (int x = 0; x < t.w; ++x) {
+                    const float* p = texels + t.offset + 3 * ((size_t)y * t.w + x);
+                    sum += (p[0] + p[1] + p[2]) / 3.f;
+                }
+            l.pdf_norm = sum / (float)(t.w * t.h);
+        }
+        return l;
+    }
     if (d.type == AUR_LIGHT_SQUARE) {
         l.xs = d.size_x;
         l.ys = d.size_y;
@@ -106,6 +127,8 @@ DevScene aur_scene::dev() const {
     d.sh.corner_uv = corner_uv;
     d.sh.tri_attr = bvh.tri_attr;
     d.sh.nlights = (int)h_lights.size();
+    d.sh.nenv = 0;
+    for (const Light& l : h_lights) d.sh.nenv += l.type == LIGHT_ENV ? 1 : 0;
     d.cam = cam;
     return d;
 }
@@ -155,9 +178,19 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     }
     std::vector<Light> lights(d->nlight);
     for (uint32_t l = 0; l < d->nlight; ++l) {
-        if (d->lights[l].type != AUR_LIGHT_SQUARE && d->lights[l].type != AUR_LIGHT_SPHERE)
+        const aur_light_desc& ld = d->lights[l];
+        if (ld.type != AUR_LIGHT_SQUARE && ld.type != AUR_LIGHT_SPHERE && ld.type != AUR_LIGHT_ENV)
             return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: unknown light type");
-        lights[l] = make_light(d->lights[l]);
+        if (ld.type == AUR_LIGHT_ENV) {
+            float inv[16];
+            if (!invert4_gj(ld.object_to_camera, inv))
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: singular camera-to-world matrix");
+            if (ld.tex >= (int)d->ntex || ld.tex < -1)
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: environment texture index");
+            if (ld.tex >= 0 && is_device_ptr(d->texels))
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: an env map needs host texels");
+        }
+        lights[l] = make_light(ld, texs, d->texels);
     }
 
     DeviceGuard g(ctx->device);

@@ -9,13 +9,14 @@
 //   renderCam  fov (slope factor, camera.cpp:51-52), transforms (camera to world)
 //   shaders    texture2DShader (texture files in PFM; EXR needs OpenEXR, not in this build)
 //   materials  matteMaterial, kelemenMaterial, metalMaterial, glassMaterial
-//   objects    geometry (OBJ triangles, optional Loop subdivision), light (square)
+//   objects    geometry (OBJ triangles, optional Loop subdivision), light (square), envlight
 //
 // Objects of a JSON object are visited in key order, as the reference's JSON
 // library (an ordered map) visits them, so global triangle ids and attribute
 // indices follow the reference's append order. Transforms use the reference's
 // FP32 matrix arithmetic (core/transform.cpp:36-136, core/matrix4x4.cpp:49-150).
 #include "aur_capi_internal.h"
+#include "aur_host_math.h"
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -261,49 +262,7 @@ M4 mul(const M4& a, const M4& b) {        // Matrix4x4::operator* (matrix4x4.cpp
             r.m[i][j] = a.m[i][0] * b.m[0][j] + a.m[i][1] * b.m[1][j] + a.m[i][2] * b.m[2][j] + a.m[i][3] * b.m[3][j];
     return r;
 }
-// Gauss-Jordan elimination with full pivoting in FP32 (the published algorithm the
-// reference's Matrix4x4::inverse uses). Returns false for a singular matrix.
-bool inverse(const M4& in, M4* out) {
-    int indxc[4], indxr[4], ipiv[4] = {0, 0, 0, 0};
-    float a[4][4];
-    memcpy(a, in.m, sizeof(a));
-    for (int i = 0; i < 4; ++i) {
-        int irow = -1, icol = -1;
-        float big = 0.f;
-        for (int j = 0; j < 4; ++j) {
-            if (ipiv[j] == 1) continue;
-            for (int k = 0; k < 4; ++k) {
-                if (ipiv[k] == 0) {
-                    if (fabsf(a[j][k]) >= big) { big = fabsf(a[j][k]); irow = j; icol = k; }
-                } else if (ipiv[k] > 1) {
-                    return false;
-                }
-            }
-        }
-        if (icol < 0) return false;
-        ++ipiv[icol];
-        if (irow != icol)
-            for (int k = 0; k < 4; ++k) std::swap(a[irow][k], a[icol][k]);
-        indxr[i] = irow;
-        indxc[i] = icol;
-        if (a[icol][icol] == 0.f) return false;
-        const float pivinv = 1.f / a[icol][icol];
-        a[icol][icol] = 1.f;
-        for (int j = 0; j < 4; ++j) a[icol][j] *= pivinv;
-        for (int j = 0; j < 4; ++j) {
-            if (j == icol) continue;
-            const float save = a[j][icol];
-            a[j][icol] = 0.f;
-            for (int k = 0; k < 4; ++k) a[j][k] -= a[icol][k] * save;
-        }
-    }
-    for (int j = 3; j >= 0; --j) {
-        if (indxr[j] == indxc[j]) continue;
-        for (int k = 0; k < 4; ++k) std::swap(a[k][indxr[j]], a[k][indxc[j]]);
-    }
-    memcpy(out->m, a, sizeof(a));
-    return true;
-}
+bool inverse(const M4& in, M4* out) { return invert4_gj(&in.m[0][0], &out->m[0][0]); }
 
 struct Xform {
     M4 m = identity(), inv = identity();
@@ -1002,6 +961,7 @@ struct Loader {
         aur_light_desc l;
         memset(&l, 0, sizeof(l));
         l.type = AUR_LIGHT_SQUARE;
+        l.tex = -1;
         for (int i = 0; i < 4; ++i)
             for (int j = 0; j < 4; ++j) l.object_to_camera[4 * i + j] = o2c.m.m[i][j];
         l.size_x = (float)need_num(o, "scaleX", where);
@@ -1022,6 +982,42 @@ struct Loader {
         append_mesh(P, idx, N, {}, attr);
         const float inten = powf(2.f, l.exposure);
         out.attr_emission.insert(out.attr_emission.end(), {l.color[0] * inten, l.color[1] * inten, l.color[2] * inten});
+    }
+
+    // getEnvLight + InfiniteAreaLight (jsonParser.cpp:262-280, infiniteAreaLight.cpp:21-33): the
+    // map is looked up in world directions through the camera-to-world transform
+    void env_light(const JValue& o, const std::string& key, const Xform& cam_to_world, int attr) {
+        const std::string where = "envlight \"" + key + "\"";
+        parse_transforms(o.get("transforms"), where);   // read and checked, as the reference reads them
+        aur_light_desc l;
+        memset(&l, 0, sizeof(l));
+        l.type = AUR_LIGHT_ENV;
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) l.object_to_camera[4 * i + j] = cam_to_world.m.m[i][j];
+        l.exposure = (float)need_num(o, "exposure", where);
+        double c[3];
+        need_nums(o, "color", 3, c, where);
+        for (int i = 0; i < 3; ++i) l.color[i] = (float)c[i];
+        l.tex = -1;
+        const std::string map = need_str(o, "envmap", where);
+        if (!map.empty()) {
+            const std::string path = resolve(dir, map);
+            const size_t dot = path.find_last_of('.');
+            const std::string ext = dot == std::string::npos ? "" : path.substr(dot);
+            if (ext != ".pfm" && ext != ".PFM")
+                throw_load(AUR_ERR_UNSUPPORTED, where + ": env map " + path + " is not a PFM file (EXR needs OpenEXR, "
+                                                "which this build does not include)");
+            std::vector<float> rgb;
+            int w = 0, h = 0;
+            read_pfm(path, &rgb, &w, &h);
+            l.tex = (int32_t)(out.tex_dims.size() / 2);
+            out.tex_dims.push_back(w);
+            out.tex_dims.push_back(h);
+            out.texels.insert(out.texels.end(), rgb.begin(), rgb.end());
+        }
+        out.lights.push_back(l);
+        out.attr_emission.insert(out.attr_emission.end(), {1.f, 1.f, 1.f});   // InfiniteAreaLight::emission()
+        (void)attr;
     }
 
     void load(const std::string& path) {
@@ -1071,8 +1067,7 @@ struct Loader {
             const std::string type = need_str(kv.second, "type", "object \"" + kv.first + "\"");
             if (type == "geometry") geo.emplace_back(kv.first, &kv.second);
             else if (type == "light") lights.emplace_back(kv.first, &kv.second);
-            else if (type == "envlight")
-                throw_load(AUR_ERR_UNSUPPORTED, "object \"" + kv.first + "\": environment lights are not built");
+            else if (type == "envlight") lights.emplace_back(kv.first, &kv.second);
             // unknown types are skipped, as the reference warns and skips them
         }
         if (geo.empty()) throw_load(AUR_ERR_PARSE, "no geometry objects");
@@ -1088,7 +1083,8 @@ struct Loader {
         out.materials.push_back(black);
         for (auto& l : lights) {
             out.attr_material.push_back(constant);
-            light(*l.second, l.first, inv_cam, attr++);
+            if (need_str(*l.second, "type", "object") == "envlight") env_light(*l.second, l.first, cam_to_world, attr++);
+            else light(*l.second, l.first, inv_cam, attr++);
         }
         if (out.tri_vidx.size() / 3 >= (1u << 30)) throw_load(AUR_ERR_UNSUPPORTED, "more than 2^30 triangles");
     }

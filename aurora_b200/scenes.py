@@ -264,6 +264,7 @@ class SceneBuilder:
         o2c = self.w2c @ object_to_world
         ld = _abi.LightDesc()
         ld.type = _abi.LIGHT_SQUARE
+        ld.tex = -1
         for k, v in enumerate(o2c.astype(F32).ravel()):
             ld.object_to_camera[k] = v
         ld.size_x, ld.size_y = size_x, size_y
@@ -284,6 +285,7 @@ class SceneBuilder:
         c = (self.w2c @ np.append(np.asarray(center_world, np.float64), 1.0))[:3]
         ld = _abi.LightDesc()
         ld.type = _abi.LIGHT_SPHERE
+        ld.tex = -1
         ld.center = _abi.f3(*c.astype(F32))
         ld.radius = radius
         ld.color = _abi.f3(*color)
@@ -293,6 +295,19 @@ class SceneBuilder:
         cn = v[f].astype(F32).reshape(-1, 9)
         em = (np.array(color, F32) * F32(2.0 ** exposure)).astype(F32)
         self.lights.append((ld, vc, f, cn, em))
+
+    def env_light(self, color=(1.0, 1.0, 1.0), exposure=0.0, texture=None):
+        """InfiniteAreaLight: a constant colour, or a latitude-longitude env map (H, W, 3; row 0 is
+        up) looked up in world directions. No geometry."""
+        ld = _abi.LightDesc()
+        ld.type = _abi.LIGHT_ENV
+        c2w = np.linalg.inv(self.w2c).astype(F32)
+        for k, v in enumerate(c2w.ravel()):
+            ld.object_to_camera[k] = v
+        ld.color = _abi.f3(*color)
+        ld.exposure = exposure
+        ld.tex = -1 if texture is None else self.texture(texture)
+        self.lights.append((ld, None, None, None, np.ones(3, F32)))   # emission() = 1, unused
 
     def build(self, render=None) -> SceneData:
         const = len(self.materials)
@@ -304,6 +319,8 @@ class SceneBuilder:
             verts.append(vc); faces.append(f + base); attr.append(np.full(len(f), i, np.int32))
             cn.append(n); cu.append(u); base += len(vc)
         for j, (ld, vc, f, n, em) in enumerate(self.lights):
+            if vc is None:      # environment light: an attribute but no shape
+                continue
             verts.append(vc); faces.append(f + base); attr.append(np.full(len(f), nobj + j, np.int32))
             cn.append(n); cu.append(np.zeros((len(f), 6), F32)); base += len(vc)
         attr_mat = np.array([o[4] for o in self.objects] + [const] * len(self.lights), np.int32)
@@ -409,17 +426,22 @@ def box_scene(width=256, height=256, spp=16, max_depth=5, seed=1, rng_seed=None,
     return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))
 
 
-def sphere_scene(width=512, height=512, spp=64, max_depth=6, seed=2, ground_texture=None) -> SceneData:
+def sphere_scene(width=512, height=512, spp=64, max_depth=6, seed=2, ground_texture=None, env=None,
+                 sphere_mat=None) -> SceneData:
     """Icosphere (5 subdivisions, 20480 tris, radius 1) with a Kelemen material (roughness 0.2,
     reflectance 0.5, diffuse 0.6) on a 10x10 Lambert 0.5 ground, lit by one quad light and one
-    sphere light. Roulette off."""
+    sphere light. Roulette off. `env` adds an environment light (SceneBuilder.env_light
+    arguments); `sphere_mat` replaces the sphere's material (_mat arguments)."""
     b = SceneBuilder(width, height, FOV40, world_to_camera=look_at((0, 1.2, 5.0), (0, 0, 0)), name="sphere")
     tex = -1
     if ground_texture is not None:
         tex = b.texture(ground_texture)
     m_ground = b.material(_abi.MAT_MATTE, diffuse=(0.5, 0.5, 0.5), diffuse_tex=tex)
-    m_sphere = b.material(_abi.MAT_KELEMEN, diffuse=(0.6, 0.6, 0.6), specular=(1.0, 1.0, 1.0), roughness=0.2,
-                          reflectance=0.5)
+    if sphere_mat is None:
+        m_sphere = b.material(_abi.MAT_KELEMEN, diffuse=(0.6, 0.6, 0.6), specular=(1.0, 1.0, 1.0), roughness=0.2,
+                              reflectance=0.5)
+    else:
+        m_sphere = b.material(**sphere_mat)
     gv = np.array([[-5, -1, 5], [5, -1, 5], [5, -1, -5], [-5, -1, -5]], np.float64)
     guv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float64)
     b.mesh(gv, np.array([[0, 1, 2], [0, 2, 3]]), m_ground, normals=np.tile([0, 1, 0], (4, 1)), uvs=guv)
@@ -427,6 +449,8 @@ def sphere_scene(width=512, height=512, spp=64, max_depth=6, seed=2, ground_text
     b.mesh(v, f, m_sphere, normals=v)
     b.square_light(translate(-2.0, 3.0, 1.0) @ rot_x(-90.0), 0.5, 0.5, (8.0, 8.0, 8.0), 0.0)
     b.sphere_light((2.2, 1.2, 1.5), 0.3, (30.0, 24.0, 18.0), 0.0)
+    if env is not None:
+        b.env_light(**env)
     return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))
 
 

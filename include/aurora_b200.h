@@ -117,7 +117,7 @@ enum {
     AUR_MAT_CONSTANT = 4,
     AUR_MAT_GLASS = 5      /* glassMaterial: specular mirror / transmission (glassMaterial.cpp:33-56) */
 };
-enum { AUR_LIGHT_SQUARE = 0, AUR_LIGHT_SPHERE = 1 };
+enum { AUR_LIGHT_SQUARE = 0, AUR_LIGHT_SPHERE = 1, AUR_LIGHT_ENV = 2 };
 
 typedef struct aur_material_desc {
     int32_t type;
@@ -138,7 +138,11 @@ typedef struct aur_material_desc {
 /* Square light: Aurora/src/lights/squareLight.{h,cpp}; the quad
  * [-size_x,size_x] x [-size_y,size_y] at z=0 mapped by object_to_camera
  * (row-major 4x4, as Transform::m). Sphere light: extension (centre and
- * radius in camera space). Radiance = color * 2^exposure. */
+ * radius in camera space). Environment light: InfiniteAreaLight
+ * (geometry/infiniteAreaLight.cpp:21-106), object_to_camera holds the
+ * CAMERA-TO-WORLD matrix (the render camera's transform; the env map is looked
+ * up in world directions), tex an env-map texture (latitude-longitude, row 0 =
+ * up) or -1 for the constant color. Radiance = color (or texel) * 2^exposure. */
 typedef struct aur_light_desc {
     int32_t type;
     float object_to_camera[16];
@@ -147,6 +151,7 @@ typedef struct aur_light_desc {
     float radius;
     float color[3];
     float exposure;
+    int32_t tex;           /* environment light: env-map texture index, -1 = constant colour */
 } aur_light_desc;
 
 /* Flattened camera-space scene, the product of
@@ -214,8 +219,8 @@ typedef struct aur_render_opts {
  * (matteMaterial, kelemenMaterial, metalMaterial), objects (geometry: OBJ
  * triangles with optional Loop subdivision, objTriangleMesh.cpp:26-92 and
  * loopSubdivMesh.cpp:167-744; light: square lights). Relative paths resolve
- * against the file's directory. Environment lights, normal maps and triplanar
- * shaders return AUR_ERR_UNSUPPORTED.
+ * against the file's directory; env maps are PFM files too. Normal maps and
+ * triplanar shaders return AUR_ERR_UNSUPPORTED.
  * aur_scene_file_read flattens the file on the host (no device work) into
  * arrays owned by the aur_scene_file; aur_scene_file_desc points a scene
  * description at them and fills *opts (may be NULL) from "options"

@@ -158,6 +158,9 @@ struct Mat {
 struct Light {
     int type; float xScale, yScale, radius; Point pCam[4]; Vector lightN; Color le; Point center; float m[16];
     Point tri[2][3];
+    // environment light (InfiniteAreaLight): m = camera-to-world, minv = world-to-camera,
+    // env map texture (or -1), 2^exposure, mean texel luminance
+    float minv[16]; int tex; float escale; float pdfNorm;
 };
 struct Tex { int w, h; const float* px; size_t offset; };   // offset: first float in the texel array
 
@@ -604,6 +607,52 @@ static BrdfState getBrdf(const Scene& sc, int matId, const Vector& Vn, const Vec
 }
 
 // ------------------------------------------------------------ lights (squareLight.h:57-122) + sphere extension
+// Matrix4x4::inverse (core/matrix4x4.cpp:77-150): Gauss-Jordan with full pivoting, FP32
+static bool invert4(const float* in, float* out) {
+    int indxc[4], indxr[4];
+    int ipiv[4] = {0, 0, 0, 0};
+    float minv[4][4];
+    memcpy(minv, in, 16 * sizeof(float));
+    for (int i = 0; i < 4; i++) {
+        int irow = -1, icol = -1;
+        float big = 0.;
+        for (int j = 0; j < 4; j++) {
+            if (ipiv[j] != 1) {
+                for (int k = 0; k < 4; k++) {
+                    if (ipiv[k] == 0) {
+                        if (fabsf(minv[j][k]) >= big) { big = float(fabsf(minv[j][k])); irow = j; icol = k; }
+                    } else if (ipiv[k] > 1) {
+                        return false;
+                    }
+                }
+            }
+        }
+        if (icol < 0) return false;
+        ++ipiv[icol];
+        if (irow != icol) for (int k = 0; k < 4; ++k) std::swap(minv[irow][k], minv[icol][k]);
+        indxr[i] = irow;
+        indxc[i] = icol;
+        if (minv[icol][icol] == 0.) return false;
+        float pivinv = 1.f / minv[icol][icol];
+        minv[icol][icol] = 1.f;
+        for (int j = 0; j < 4; j++) minv[icol][j] *= pivinv;
+        for (int j = 0; j < 4; j++) {
+            if (j != icol) {
+                float save = minv[j][icol];
+                minv[j][icol] = 0;
+                for (int k = 0; k < 4; k++) minv[j][k] -= minv[icol][k] * save;
+            }
+        }
+    }
+    for (int j = 3; j >= 0; j--) {
+        if (indxr[j] != indxc[j]) {
+            for (int k = 0; k < 4; k++) std::swap(minv[k][indxr[j]], minv[k][indxc[j]]);
+        }
+    }
+    memcpy(out, minv, 16 * sizeof(float));
+    return true;
+}
+
 static Point xformPoint(const float* m, const Point& p) {     // transform.cpp:196-204
     float xp = m[0] * p.x + m[1] * p.y + m[2] * p.z + m[3];
     float yp = m[4] * p.x + m[5] * p.y + m[6] * p.z + m[7];
@@ -612,7 +661,45 @@ static Point xformPoint(const float* m, const Point& p) {     // transform.cpp:1
     if (wp == 1.f) return Point(xp, yp, zp);
     return Point(xp, yp, zp) / wp;
 }
+// ---- environment light (geometry/infiniteAreaLight.cpp:35-106, frontend/texture2D.cpp)
+static Vector xformVector(const float* m, const Vector& v) {      // transform.cpp:222-228
+    return Vector(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
+                  m[8] * v.x + m[9] * v.y + m[10] * v.z);
+}
+static int envTexel(const Tex& t, float s, float tt) {           // Texture2D::read / ::pdf, filter 0
+    int x = (int)floorf(s * t.w);
+    int y = (int)floorf(tt * t.h);
+    if (y == t.h) y -= 1;
+    if (x == t.w) x -= 1;
+    x = std::max(0, std::min(x, t.w - 1));
+    y = std::max(0, std::min(y, t.h - 1));
+    return y * t.w + x;
+}
+static Color envRead(const Scene& sc, const Light& l, float s, float tt) {
+    const Tex& t = sc.texs[l.tex];
+    const float* p = t.px + 3 * envTexel(t, s, tt);
+    return Color(p[0], p[1], p[2]);
+}
+static float envMapPdf(const Scene& sc, const Light& l, float s, float tt) {   // p.a / m_pdf_normalization
+    Color c = envRead(sc, l, s, tt);
+    return ((c.r + c.g + c.b) / 3.f) / l.pdfNorm;
+}
+static void envUV(const Light& l, const Vector& camDir, float* u, float* v) {
+    Vector dir = xformVector(l.m, camDir);
+    *v = 0.5 * (1.f - dir.y);
+    float uu = atan2f(dir.z, dir.x) / (M_PI * 2.f);
+    if (uu < 0.f) uu += 1.f;
+    *u = uu;
+}
+static Color lightEval(const Scene& sc, const Light& l, const Vector& dir) {    // Light::eval
+    if (l.type != AUR_LIGHT_ENV || l.tex < 0) return l.le;
+    float u, v;
+    envUV(l, dir, &u, &v);
+    return envRead(sc, l, u, v) * l.escale;
+}
+
 static bool lightVisible(const Light& l, const Point& P, const Vector& Nn) {
+    if (l.type == AUR_LIGHT_ENV) return true;
     if (l.type == AUR_LIGHT_SQUARE) {
         for (int i = 0; i < 4; ++i) if (dot(l.pCam[i] - P, Nn) > 0.f) return true;
         return false;
@@ -636,8 +723,30 @@ static bool sphereHit(const Light& l, const Point& o, const Vector& d, float min
     *t = tt;
     return tt >= mint;
 }
-static Sample3D lightGenerateSample(const Light& l, const Point& orig, float x, float y) {
+static Sample3D lightGenerateSample(const Scene& sc, const Light& l, const Point& orig, const Vector& Nn, float x,
+                                    float y) {
     Sample3D s;
+    if (l.type == AUR_LIGHT_ENV) {                                  // InfiniteAreaLight::generateSample
+        Vector dirW;
+        float pdf = 1.f;
+        if (l.tex >= 0) {
+            float vy = 1.f - 2.f * y;
+            float r = sqrtf(std::max(0.f, 1.f - vy * vy));
+            float phi = 2.f * M_PI * x;
+            float vx = r * cosf(phi);
+            float vz = r * sinf(phi);
+            dirW = xformVector(l.minv, Vector(vx, vy, vz));
+            pdf = envMapPdf(sc, l, x, y);
+        } else {
+            pdf = 2.f;
+            Vector dirT = SampleHemisphereUniform(x, y);
+            dirW = tangentToWorld(dirT, Nn);
+        }
+        s.ray.direction = normalize(dirW); s.ray.origin = orig; s.ray.mint = RAY_BIAS; s.ray.maxt = 1000000.f;
+        s.pdf = pdf / (M_PI * 4.);
+        s.color = lightEval(sc, l, s.ray.direction);
+        return s;
+    }
     if (l.type == AUR_LIGHT_SQUARE) {
         Point lightP((x - 0.5) * l.xScale * 2, (y - 0.5) * l.yScale * 2, 0.f);
         lightP = xformPoint(l.m, lightP);
@@ -669,7 +778,14 @@ static Sample3D lightGenerateSample(const Light& l, const Point& orig, float x, 
     s.pdf = solid > 0.f ? 1.f / solid : 0.f;
     return s;
 }
-static float lightPdf(const Light& l, Ray* ray) {        // SquareLight::pdf (squareLight.h:88-97)
+static float lightPdf(const Scene& sc, const Light& l, Ray* ray) {   // SquareLight::pdf (squareLight.h:88-97)
+    if (l.type == AUR_LIGHT_ENV) {                                  // InfiniteAreaLight::pdf, hemisphere
+        if (l.tex < 0) return 1.f / (M_PI * 2.f);
+        float u, v;
+        envUV(l, ray->direction, &u, &v);
+        float pdf = envMapPdf(sc, l, u, v);
+        return pdf / (M_PI * 2.f);
+    }
     if (l.type == AUR_LIGHT_SQUARE) {
         float t, b1, b2;
         bool hit = triIntersect(l.tri[0][0], l.tri[0][1], l.tri[0][2], *ray, &t, &b1, &b2);
@@ -764,7 +880,7 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
     const Light& light = sc.lights[idx[k]];
     float lx = rng(vdim(vtx, DIM_LIGHTSAMPLE)), ly = rng(vdim(vtx, DIM_LIGHTSAMPLE + 1));
     if (brdf.type == MatteBrdf) {                                         // integrateDirectLight :33-54
-        Sample3D ls = lightGenerateSample(light, lg.P, lx, ly);
+        Sample3D ls = lightGenerateSample(sc, light, lg.P, lg.Nn, lx, ly);
         float costheta = dot(lg.Nn, ls.ray.direction);
         if (costheta >= 0. && ls.pdf > 0.) {
             ++cnt.shadow;
@@ -777,7 +893,7 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
             }
         }
     } else if (brdf.type == SpecBrdf) {                                   // integrateDirectMIS :56-98
-        Sample3D ls = lightGenerateSample(light, lg.P, lx, ly);
+        Sample3D ls = lightGenerateSample(sc, light, lg.P, lg.Nn, lx, ly);
         float costheta = dot(lg.Nn, ls.ray.direction);
         if (costheta > 0. && ls.pdf > 0.) {
             float bp = brdfPdf(brdf, ls.ray.direction, lg.Vn, lg.Nn);
@@ -801,12 +917,12 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
         bs.ray.origin = lg.P;
         costheta = dot(lg.Nn, bs.ray.direction);
         if (costheta > 0.) {
-            float lp = lightPdf(light, &bs.ray);
+            float lp = lightPdf(sc, light, &bs.ray);
             if (lp > 0. && bs.pdf > 0.) {
                 ++cnt.shadow;
                 if (!sceneOccluded(sc, bs.ray)) {
                     float weight = PowerHeuristic(1, bs.pdf, 1, lp);
-                    Color c1 = bs.color * weight * light.le * costheta / bs.pdf;
+                    Color c1 = bs.color * weight * lightEval(sc, light, bs.ray.direction) * costheta / bs.pdf;
                     result += c1;
                     if (grad) {
                         const double g = dlnBeckmannSampled(brdf, bs.ray.direction, lg.Vn, lg.Nn);
@@ -827,10 +943,16 @@ enum { CameraRay = 0, DiffuseRay = 1, SpecularRay = 2, MirrorRay = 3 };
 static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng, int maxDepth, int minDepth,
                                    float* alpha, Counts& cnt) {
     Ray ray = convertSample(sc, x, y, rng(0), rng(1));
+    const Vector camDir = ray.direction;
     *alpha = 0;
     ++cnt.closest;
     int prim; float t, u, v;
-    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) return Color(0.f);
+    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {   // camera miss: the environment lights (integrator.cpp:290-300)
+        Color env(0.f);
+        for (const Light& l : sc.lights)
+            if (l.type == AUR_LIGHT_ENV) { env += lightEval(sc, l, camDir); *alpha = 1.f; }
+        return env;
+    }
     *alpha = 1.f;
     Color Lo(0.f);
     float continueProbability = 1.f;
@@ -867,7 +989,14 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
         if (trueBounces >= maxDepth) break;   // unshaded last ray skipped (no environment lights)
         ray = cur.ray;
         ++cnt.closest;
-        if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) break;
+        if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {
+            // a mirror ray that escapes adds the environment along the CAMERA sample's
+            // direction (integrator.cpp:262-274 evaluates `sample`, the camera ray)
+            if (rayType == MirrorRay)
+                for (const Light& l : sc.lights)
+                    if (l.type == AUR_LIGHT_ENV) Lo += lightEval(sc, l, camDir) * pathThroughput;
+            break;
+        }
     }
     // firefly filter; a non-finite estimate (which would never leave the loop) is dropped
     if (!std::isfinite(Lo.r) || !std::isfinite(Lo.g) || !std::isfinite(Lo.b)) return Color(0.f);
@@ -942,12 +1071,33 @@ static void addDT(std::vector<DThroughput>& dT, long base, bool perChannel, cons
 
 // One camera path: the forward arithmetic of integrateCameraSample, plus the derivative
 // of <delta, L> added (times the firefly factor) to grad.
+// A mirror ray that escapes: Lo += E T for every environment light along the camera
+// direction, and its derivative dT E.
+static void envMiss(const Scene& sc, const Vector& camDir, const Color& T, const std::vector<DThroughput>& dT,
+                    const double delta[3], Color& Lo, std::vector<std::pair<long, double>>& contrib) {
+    for (const Light& l : sc.lights) {
+        if (l.type != AUR_LIGHT_ENV) continue;
+        const Color E = lightEval(sc, l, camDir);
+        Lo += E * T;
+        for (const auto& e : dT) {
+            if (e.perChannel) {
+                contrib.push_back({e.base + 0, delta[0] * e.d[0] * E.r});
+                contrib.push_back({e.base + 1, delta[1] * e.d[1] * E.g});
+                contrib.push_back({e.base + 2, delta[2] * e.d[2] * E.b});
+            } else {
+                contrib.push_back({e.base, delta[0] * e.d[0] * E.r + delta[1] * e.d[1] * E.g + delta[2] * e.d[2] * E.b});
+            }
+        }
+    }
+}
+
 static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, int maxDepth, int minDepth,
                                 const double delta[3], double* grad) {
     Counts cnt;
     Ray ray = convertSample(sc, x, y, rng(0), rng(1));
+    const Vector camDir = ray.direction;
     int prim; float t, u, v;
-    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) return;
+    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) return;   // the environment alone: no parameter
     Color Lo(0.f);
     float continueProbability = 1.f;
     Color pathThroughput(1.f);
@@ -1013,7 +1163,10 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
             ++trueBounces;
             if (trueBounces >= maxDepth) break;
             ray = cur.ray;
-            if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) break;
+            if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {
+                if (rayType == MirrorRay) envMiss(sc, camDir, pathThroughput, dT, delta, Lo, contrib);
+                break;
+            }
             continue;
         }
         const float cosl = dot(lg.Nn, cur.ray.direction);
@@ -1047,7 +1200,10 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         ++bounces;
         if (trueBounces >= maxDepth) break;
         ray = cur.ray;
-        if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) break;
+        if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {
+                if (rayType == MirrorRay) envMiss(sc, camDir, pathThroughput, dT, delta, Lo, contrib);
+                break;
+            }
     }
     if (!std::isfinite(Lo.r) || !std::isfinite(Lo.g) || !std::isfinite(Lo.b)) return;   // dropped, as the forward
     double clamp = 1.0;
@@ -1093,7 +1249,13 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
         float intensity = powf(2, ld.exposure);
         l.le = Color(ld.color[0], ld.color[1], ld.color[2]) * intensity;
         memcpy(l.m, ld.object_to_camera, sizeof(l.m));
-        if (ld.type == AUR_LIGHT_SQUARE) {
+        l.tex = -1;
+        if (ld.type == AUR_LIGHT_ENV) {                 // InfiniteAreaLight ctor; m = camera-to-world
+            l.escale = pow(2, ld.exposure);             // eval: color * pow(2, m_exposure)
+            l.le = Color(ld.color[0], ld.color[1], ld.color[2]) * l.escale;
+            invert4(l.m, l.minv);
+            l.tex = ld.tex;                             // pdf normalisation once the texels are in
+        } else if (ld.type == AUR_LIGHT_SQUARE) {
             l.xScale = ld.size_x; l.yScale = ld.size_y;
             Point p1 = xformPoint(l.m, Point(-l.xScale, -l.yScale, 0));
             Point p2 = xformPoint(l.m, Point(-l.xScale, l.yScale, 0));
@@ -1119,6 +1281,17 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
     sc->texels.assign(d->texels ? d->texels : nullptr, d->texels ? d->texels + off : nullptr);
     off = 0;
     for (auto& tx : sc->texs) { tx.px = sc->texels.data() + off; off += 3 * (size_t)tx.w * tx.h; }
+    for (auto& l : sc->lights) {                        // Texture2D::initPdf: m_pdf_normalization
+        if (l.type != AUR_LIGHT_ENV || l.tex < 0) continue;
+        const Tex& t = sc->texs[l.tex];
+        float lum = 0;
+        for (int i = 0; i < t.h; i++)
+            for (int j = 0; j < t.w; j++) {
+                const float* p = t.px + 3 * ((size_t)i * t.w + j);
+                lum += (p[0] + p[1] + p[2]) / 3.f;
+            }
+        l.pdfNorm = lum / (t.w * t.h);
+    }
     sc->albedo = albedo;
     sc->fov = d->fov; sc->width = d->width; sc->height = d->height;
     return sc;
@@ -1341,12 +1514,12 @@ int oracle_kelemen_table(float reflectance, int samples, uint32_t seed, float* o
 // kind 3 kelemen       in: table index, costheta, roughness          (3) out: albedo (1)
 // kind 4 camera_ray    in: fov, w, h, px, py, j1, j2                 (7) out: dir3 (3)
 // kind 5 power_heur.   in: f, g                                      (2) out: w (1)
-// kind 6 light_sample  in: light, P3, u1, u2                         (6) out: dir3, maxt, pdf, color3 (8)
+// kind 6 light_sample  in: light, P3, u1, u2, N3                     (9) out: dir3, maxt, pdf, color3 (8)
 // kind 7 light_pdf     in: light, o3, d3, mint, maxt                 (9) out: pdf, maxt (2)
 // kind 8 light_visible in: light, P3, N3                             (7) out: visible (1)
 // kind 9 get_brdf      in: material, V3, N3, su, sv, matte, lobe_u  (11) out: lobe, color3, rough (5)
 int oracle_shading_probe(void* h, int kind, const float* in, uint32_t n, float* out, const float* tables) {
-    static const int kIn[10] = {13, 14, 14, 3, 7, 2, 6, 9, 7, 11};
+    static const int kIn[10] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11};
     static const int kOut[10] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5};
     if (kind < 0 || kind > 9) return -1;
     const Scene* sc = (const Scene*)h;
@@ -1374,12 +1547,13 @@ int oracle_shading_probe(void* h, int kind, const float* in, uint32_t n, float* 
         } else if (kind == 5) {
             o[0] = PowerHeuristic(1, q[0], 1, q[1]);
         } else if (kind == 6) {
-            Sample3D s = lightGenerateSample(sc->lights[(int)q[0]], Point(q[1], q[2], q[3]), q[4], q[5]);
+            Sample3D s = lightGenerateSample(*sc, sc->lights[(int)q[0]], Point(q[1], q[2], q[3]), Vector(q[6], q[7], q[8]),
+                                             q[4], q[5]);
             o[0] = s.ray.direction.x; o[1] = s.ray.direction.y; o[2] = s.ray.direction.z; o[3] = s.ray.maxt;
             o[4] = s.pdf; o[5] = s.color.r; o[6] = s.color.g; o[7] = s.color.b;
         } else if (kind == 7) {
             Ray r; r.origin = Point(q[1], q[2], q[3]); r.direction = Vector(q[4], q[5], q[6]); r.mint = q[7]; r.maxt = q[8];
-            o[0] = lightPdf(sc->lights[(int)q[0]], &r); o[1] = r.maxt;
+            o[0] = lightPdf(*sc, sc->lights[(int)q[0]], &r); o[1] = r.maxt;
         } else if (kind == 8) {
             o[0] = lightVisible(sc->lights[(int)q[0]], Point(q[1], q[2], q[3]), Vector(q[4], q[5], q[6])) ? 1.f : 0.f;
         } else {

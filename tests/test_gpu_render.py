@@ -69,6 +69,32 @@ def test_glass_boxes(ctx, oracle_lib, kelemen_tables, mode):
     compare(g, mean, m2, 16)
 
 
+ENV_MAP = np.random.default_rng(15).uniform(0.05, 4.0, (32, 64, 3)).astype(np.float32)
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+@pytest.mark.parametrize("env", [dict(color=(0.4, 0.5, 0.7), exposure=0.0),
+                                 dict(color=(1, 1, 1), exposure=-1.0, texture=ENV_MAP)], ids=["constant", "map"])
+def test_environment_light(ctx, oracle_lib, kelemen_tables, mode, env):
+    """InfiniteAreaLight: seen by camera rays that miss (alpha 1), sampled by next-event
+    estimation and weighted against BRDF samples by MIS, and seen through a glass sphere by
+    mirror rays that escape (evaluated along the camera ray, as the reference does)."""
+    from aurora_b200 import scenes
+    glass = dict(type_=5, specular=(1.0, 1.0, 1.0), diffuse=(0.9, 0.95, 1.0), reflectance=0.04, ior=1.5)
+    data = scenes.sphere_scene(96, 96, env=env, sphere_mat=glass)
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16, mode=mode)
+    compare(g, mean, m2, 16)
+    assert (mean[..., 3] == 1.0).all()     # every pixel sees geometry or the environment
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_environment_map_with_kelemen(ctx, oracle_lib, kelemen_tables, mode):
+    from aurora_b200 import scenes
+    data = scenes.sphere_scene(96, 96, env=dict(color=(1, 1, 1), exposure=0.0, texture=ENV_MAP))
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16, mode=mode)
+    compare(g, mean, m2, 16)
+
+
 def test_terrain_small(ctx, oracle_lib, kelemen_tables):
     """The large-scene generator at reduced size (roulette, 16 materials, 4 lights, depth 8)."""
     from aurora_b200 import scenes

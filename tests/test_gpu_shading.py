@@ -82,7 +82,8 @@ def test_kelemen_tables_match_restatement(kelemen_tables, oracle_lib):
 def test_lights_and_materials(ctx, oracle_lib, kelemen_tables):
     import aurora_b200 as ab
     from aurora_b200 import scenes
-    data = scenes.sphere_scene(64, 64)
+    env = np.random.default_rng(14).uniform(0.1, 3.0, (16, 32, 3)).astype(np.float32)
+    data = scenes.sphere_scene(64, 64, env=dict(color=(1, 1, 1), exposure=0.5, texture=env))   # lights: square, sphere, env
     scene = ab.Scene(ctx, data)
     osc = oracle_lib.OracleScene(data, kelemen_tables, use_bvh=False)
     r = np.random.default_rng(13)
@@ -90,7 +91,7 @@ def test_lights_and_materials(ctx, oracle_lib, kelemen_tables):
     P = r.uniform(-3, 3, (n, 3)) + scenes.sphere_center_camera(data)
     N = rand_dirs(r, n)
     li = r.integers(0, len(data.lights), n)
-    ls = np.concatenate([li[:, None], P, r.uniform(0, 1, (n, 2))], 1).astype(np.float32)
+    ls = np.concatenate([li[:, None], P, r.uniform(0, 1, (n, 2)), N], 1).astype(np.float32)
     close(ctx.probe(6, ls, scene), osc.probe(6, ls), rtol=2e-5, atol=1e-5, frac=1e-3)
     vis = np.concatenate([li[:, None], P, N], 1).astype(np.float32)
     assert np.array_equal(ctx.probe(8, vis, scene), osc.probe(8, vis))

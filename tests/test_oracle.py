@@ -244,3 +244,44 @@ def test_mirror_and_transmission_known_answers(oracle_lib):
     # an exact mirror where the frame is unit length (N orthogonal to y)
     m = oracle_lib.probe(0, np.array([[2, 1, 1, 1, 0, 0.6, 0, 0.8, 0, 0, 1, 0.5, 0.5]], np.float32))
     np.testing.assert_allclose(m[0, :3], [-0.6, 0, 0.8], atol=1e-7)
+
+
+def _plane_under_sky(env, albedo=0.5):
+    """A Lambert plane filling the view under an environment light (nothing else)."""
+    from aurora_b200 import _abi, scenes
+    b = scenes.SceneBuilder(32, 32, 0.3, world_to_camera=scenes.look_at((0, 3, 0.01), (0, 0, 0)), name="plane")
+    m = b.material(_abi.MAT_MATTE, diffuse=(albedo, albedo, albedo))
+    v = np.array([[-50, 0, 50], [50, 0, 50], [50, 0, -50], [-50, 0, -50]], np.float64)
+    b.mesh(v, np.array([[0, 1, 2], [0, 2, 3]]), m, normals=np.tile([0, 1.0, 0], (4, 1)))
+    b.env_light(**env)
+    return b.build(render=dict(spp=64, max_depth=1, min_depth=1, seed=3))
+
+
+@pytest.mark.parametrize("env", [dict(color=(2.0, 1.0, 0.5), exposure=1.0),
+                                 dict(color=(1, 1, 1), exposure=0.0,
+                                      texture=np.full((16, 32, 3), 1.5, np.float32))],
+                         ids=["constant", "uniform-map"])
+def test_env_light_lambert_plane(oracle_lib, env):
+    """Next-event estimation of a constant sky above a Lambert plane: a*E in expectation, both
+    with uniform hemisphere sampling (pdf 1/2pi) and with the env map's uniform-sphere
+    sampling weighted by the map pdf (texel luminance / mean = 1 here, pdf 1/4pi)."""
+    from aurora_b200 import scenes
+    data = _plane_under_sky(env)
+    E = np.array(env["color"]) * 2.0 ** env["exposure"] * (1.5 if "texture" in env else 1.0)
+    mean, m2, _ = oracle_lib.OracleScene(data).render(256, 1, 1, 3)
+    got = mean[..., :3].mean((0, 1))
+    np.testing.assert_allclose(got, 0.5 * E, rtol=0.01)
+
+
+def test_env_light_seen_by_camera(oracle_lib):
+    """Camera rays that miss see the environment (alpha 1), unfiltered."""
+    from aurora_b200 import _abi, scenes
+    b = scenes.SceneBuilder(8, 8, 0.3, world_to_camera=scenes.look_at((0, 3, 0.01), (0, 0, 0)))
+    m = b.material(_abi.MAT_MATTE, diffuse=(0.5, 0.5, 0.5))
+    v = np.array([[100, -5, 100], [101, -5, 100], [100, -5, 101]], np.float64)   # out of view
+    b.mesh(v, np.array([[0, 1, 2]]), m)
+    b.env_light(color=(300.0, 2.0, 1.0))
+    data = b.build(render=dict(spp=4, max_depth=3, min_depth=3, seed=1))
+    mean, _, _ = oracle_lib.OracleScene(data).render(4, 3, 3, 1)
+    np.testing.assert_allclose(mean[..., :3], np.broadcast_to([300.0, 2.0, 1.0], (8, 8, 3)), rtol=1e-6)
+    assert np.all(mean[..., 3] == 1.0)

@@ -252,7 +252,9 @@ def test_texture_shader_and_kelemen_material(tmp_path):
     (lambda s: s["materials"].update({"m": {"type": "glassMaterial"}}), _abi.ERR_PARSE),
     (lambda s: s["materials"].update({"m": {"type": "matteMaterial", "color": [1, 1, 1], "normalmap": "n"}}),
      _abi.ERR_UNSUPPORTED),
-    (lambda s: s["objects"].update({"e": {"type": "envlight"}}), _abi.ERR_UNSUPPORTED),
+    (lambda s: s["objects"].update({"e": {"type": "envlight"}}), _abi.ERR_PARSE),
+    (lambda s: s["objects"].update({"e": {"type": "envlight", "transforms": [], "exposure": 0, "color": [1, 1, 1],
+                                          "envmap": "sky.exr"}}), _abi.ERR_UNSUPPORTED),
     (lambda s: s["objects"]["g"].update({"material": "nope"}), _abi.ERR_PARSE),
     (lambda s: s["objects"]["g"].update({"path": "missing.obj"}), _abi.ERR_IO),
     (lambda s: s["materials"]["m"].update({"color": "noshader"}), _abi.ERR_PARSE),
@@ -297,3 +299,20 @@ def test_glass_material(tmp_path):
     m = data.materials[0]
     assert m.type == _abi.MAT_GLASS and m.ior == np.float32(1.5) and m.reflectance == np.float32(0.04)
     assert tuple(m.specular) == (1, 1, 1) and np.allclose(tuple(m.diffuse), (0.9, 0.8, 0.7))
+
+
+def test_environment_light_file(tmp_path):
+    v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
+    write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
+    env = np.random.default_rng(4).uniform(0, 2, (8, 16, 3)).astype(np.float32)
+    write_pfm(str(tmp_path / "sky.pfm"), env)
+    p = write_single(str(tmp_path), "q.obj", 0, extra_objects={
+        "sky": {"type": "envlight", "name": "sky", "transforms": [], "exposure": 1.0, "color": [1, 1, 1],
+                "envmap": "sky.pfm"}})
+    data, _, _ = scenes.load_scene_file(p)
+    assert len(data.lights) == 1 and data.lights[0].type == _abi.LIGHT_ENV and data.lights[0].tex == 0
+    np.testing.assert_array_equal(data.textures[0], env)
+    # the camera-to-world matrix of the render camera (translate 0 0 5)
+    m = np.array(data.lights[0].object_to_camera).reshape(4, 4)
+    np.testing.assert_allclose(m, [[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 1, 5], [0, 0, 0, 1]])
+    assert data.attr_material[-1] == len(data.materials) - 1 and data.ntri == 2
