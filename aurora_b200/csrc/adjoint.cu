@@ -152,7 +152,7 @@ __device__ __forceinline__ float3 direct(const DevScene& sc, const Frame& f, con
     int nvis;
     const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
     if (li < 0) return res;
-    const Light L = sc.sh.lights[li];
+    const Light& L = sc.sh.lights[li];   // global: the env paths take its address
     const LightSample ls = light_sample(sc.sh, L, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightSample)),
                                         rng.u(vertex_dim(vtx, kDimLightSample + 1)));
     float cost = dot(f.N, ls.dir);

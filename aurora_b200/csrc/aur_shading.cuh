@@ -400,19 +400,38 @@ AUR_HD void env_uv(const Light& l, float3 dir_cam, float* u, float* v) {
 }
 // radiance arriving along camera-space direction `dir` from a light (Light::eval): the
 // square and sphere lights are constant, the environment reads its map
+// (the environment's paths are kept out of line: inlined, they raise the register count of
+// every shading kernel, with or without an environment in the scene)
+// (their arguments are global pointers and values: an address of a local copy or of a
+// kernel parameter would force that into local memory)
+static __host__ __device__ __noinline__ float3 env_map_eval(const Texture* texs, const float* texels, const Light* l,
+                                                            float3 dir) {
+    ShadeScene sh;
+    sh.texs = texs;
+    sh.texels = texels;
+    float u, v;
+    env_uv(*l, dir, &u, &v);
+    return env_texel(sh, l->tex, u, v) * l->escale;
+}
+// `l` must live in global memory (a reference into ShadeScene::lights)
 AUR_HD float3 light_eval(const ShadeScene& sh, const Light& l, float3 dir) {
     if (l.type != LIGHT_ENV || l.tex < 0) return l.le;
-    float u, v;
-    env_uv(l, dir, &u, &v);
-    return env_texel(sh, l.tex, u, v) * l.escale;
+    return env_map_eval(sh.texs, sh.texels, &l, dir);
 }
 // every environment light's radiance along `dir` (camera-ray and mirror-ray misses,
 // integrator.cpp:262-288)
-AUR_HD float3 env_radiance(const ShadeScene& sh, float3 dir) {
+static __host__ __device__ __noinline__ float3 env_radiance_of(const Light* lights, int n, const Texture* texs,
+                                                               const float* texels, float3 dir) {
     float3 r = mk(0.f, 0.f, 0.f);
-    for (int i = 0; i < sh.nlights; ++i)
-        if (sh.lights[i].type == LIGHT_ENV) r += light_eval(sh, sh.lights[i], dir);
+    for (int i = 0; i < n; ++i) {
+        const Light* l = &lights[i];
+        if (l->type != LIGHT_ENV) continue;
+        r += l->tex < 0 ? l->le : env_map_eval(texs, texels, l, dir);
+    }
     return r;
+}
+AUR_HD float3 env_radiance(const ShadeScene& sh, float3 dir) {
+    return env_radiance_of(sh.lights, sh.nlights, sh.texs, sh.texels, dir);
 }
 
 AUR_HD bool light_visible(const Light& l, float3 P, float3 N) {       // squareLight.h:99-110
@@ -454,9 +473,14 @@ AUR_HD float sphere_cone_cos(const Light& l, float3 P) {
     return sqrtf(fmaxf(0.f, 1.f - s2));
 }
 
-AUR_HD LightSample light_sample(const ShadeScene& sh, const Light& l, float3 P, float3 N, float u1, float u2) {
+static __host__ __device__ __noinline__ LightSample env_light_sample(const Texture* texs, const float* texels,
+                                                                    const Light* lp, float3 N, float u1, float u2) {
+    ShadeScene sh;
+    sh.texs = texs;
+    sh.texels = texels;
+    const Light& l = *lp;
     LightSample s;
-    if (l.type == LIGHT_ENV) {                                           // infiniteAreaLight.cpp:35-61
+    {                                                                    // infiniteAreaLight.cpp:35-61
         float3 dirw;
         float pdf;
         if (l.tex >= 0) {   // a uniform direction on the sphere, weighted by the map's pdf at (u1, u2)
@@ -472,9 +496,14 @@ AUR_HD LightSample light_sample(const ShadeScene& sh, const Light& l, float3 P, 
         s.dir = normalize(dirw);
         s.maxt = 1000000.f;
         s.pdf = (float)((double)pdf / 12.566370614359172);               // pdf / (M_PI * 4.)
-        s.color = light_eval(sh, l, s.dir);
+        s.color = l.tex < 0 ? l.le : env_map_eval(texs, texels, lp, s.dir);
         return s;
     }
+}
+
+AUR_HD LightSample light_sample(const ShadeScene& sh, const Light& l, float3 P, float3 N, float u1, float u2) {
+    LightSample s;
+    if (l.type == LIGHT_ENV) return env_light_sample(sh.texs, sh.texels, &l, N, u1, u2);
     if (l.type == LIGHT_SQUARE) {                                        // squareLight.h:57-82
         float3 lp = mk((float)(((double)u1 - 0.5) * l.xs * 2.0), (float)(((double)u2 - 0.5) * l.ys * 2.0), 0.f);
         lp = xform_point(l.m, lp);
@@ -510,13 +539,21 @@ AUR_HD LightSample light_sample(const ShadeScene& sh, const Light& l, float3 P, 
 
 // SquareLight::pdf (squareLight.h:88-97): hits the two light triangles, shortens
 // the ray to the light and returns the solid-angle pdf (two-sided, as in the reference).
+static __host__ __device__ __noinline__ float env_light_pdf(const Texture* texs, const float* texels, const Light* lp,
+                                                            float3 d) {
+    // infiniteAreaLight.cpp:82-106, hemisphere domain
+    const Light& l = *lp;
+    if (l.tex < 0) return (float)(1.0 / 6.283185307179586);             // 1.f / (M_PI * 2.f)
+    ShadeScene sh;
+    sh.texs = texs;
+    sh.texels = texels;
+    float u, v;
+    env_uv(l, d, &u, &v);
+    return (float)((double)env_texel_pdf(sh, l, u, v) / 6.283185307179586);
+}
+
 AUR_HD float light_pdf(const ShadeScene& sh, const Light& l, float3 o, float3 d, float mint, float* maxt) {
-    if (l.type == LIGHT_ENV) {                                           // infiniteAreaLight.cpp:82-106, hemisphere
-        if (l.tex < 0) return (float)(1.0 / 6.283185307179586);         // 1.f / (M_PI * 2.f)
-        float u, v;
-        env_uv(l, d, &u, &v);
-        return (float)((double)env_texel_pdf(sh, l, u, v) / 6.283185307179586);
-    }
+    if (l.type == LIGHT_ENV) return env_light_pdf(sh.texs, sh.texels, &l, d);
     if (l.type == LIGHT_SQUARE) {
         float t, b1, b2;
         bool hit = tri_intersect(l.p[0], xsub(l.p[1], l.p[0]), xsub(l.p[3], l.p[0]), o, d, mint, *maxt, &t, &b1, &b2);

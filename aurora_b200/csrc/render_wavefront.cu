@@ -333,6 +333,26 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
 }
 
 // ------------------------------------------------------------------ shade
+// A ray that missed in a scene with environment lights: the camera ray sees the
+// environment (alpha 1, no firefly filter), an escaping mirror ray adds it times the
+// throughput, both along the camera ray's direction (integrator.cpp:262-288). Out of line.
+__device__ __noinline__ float4 shade_env_miss(uint4* ids, const float4* tp, const WfScene* S, uint32_t slot, uint4 id,
+                                              int vtx, float4 lo) {
+    PathRng rng;
+    rng.key = S->key;
+    rng.base = path_base(id.y, (uint32_t)S->p.sample_offset + id.z);
+    const RayF cr = camera_ray(S->sc.cam, (int)(id.y % (uint32_t)S->sc.cam.w), (int)(id.y / (uint32_t)S->sc.cam.w),
+                               rng.u(kDimCamera), rng.u(kDimCamera + 1));
+    const float3 e = env_radiance_of(S->sc.sh.lights, S->sc.sh.nlights, S->sc.sh.texs, S->sc.sh.texels, cr.d);
+    if (vtx == 0) {
+        ids[slot].w = id.w | kNoClamp;
+        return make_float4(e.x, e.y, e.z, 1.f);
+    }
+    const float4 t = tp[slot];
+    const float3 a = e * mk(t.x, t.y, t.z);
+    return make_float4(lo.x + a.x, lo.y + a.y, lo.z + a.z, lo.w);
+}
+
 template <bool kRec>
 __global__ void k_shade(WfPool w, int in_q, int sorted) {
     const uint32_t* qin = sorted ? w.q_sort : (in_q ? w.q_ext1 : w.q_ext0);
@@ -362,24 +382,8 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 const uint4 id = w.id[slot];
                 const WfScene& S = w.scenes[id.x];
                 const int kind = f_kind(id.w), vtx = f_vtx(id.w);
-                if (S.sc.sh.nenv && (vtx == 0 || kind == RAY_MIRROR)) {
-                    // the environment along the camera ray (integrator.cpp:262-288)
-                    PathRng rng;
-                    rng.key = S.key;
-                    rng.base = path_base(id.y, (uint32_t)S.p.sample_offset + id.z);
-                    const RayF cr = camera_ray(S.sc.cam, (int)(id.y % (uint32_t)S.sc.cam.w),
-                                               (int)(id.y / (uint32_t)S.sc.cam.w), rng.u(kDimCamera),
-                                               rng.u(kDimCamera + 1));
-                    const float3 e = env_radiance(S.sc.sh, cr.d);
-                    if (vtx == 0) {
-                        lo = make_float4(e.x, e.y, e.z, 1.f);
-                        w.id[slot].w = id.w | kNoClamp;
-                    } else {
-                        const float4 t = w.tp[slot];
-                        const float3 a = e * mk(t.x, t.y, t.z);
-                        lo.x += a.x; lo.y += a.y; lo.z += a.z;
-                    }
-                }
+                if (S.sc.sh.nenv && (vtx == 0 || kind == RAY_MIRROR))
+                    lo = shade_env_miss(w.id, w.tp, &S, slot, id, vtx, lo);
                 w.state[slot] = PS_DONE;
             } else {
                 const uint4 id = w.id[slot];
@@ -412,7 +416,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                     int nvis;
                     const int li = pick_visible_light(sc.sh, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightPick)), &nvis);
                     if (li >= 0) {
-                        const Light L = sc.sh.lights[li];
+                        const Light& L = sc.sh.lights[li];   // global: the env paths take its address
                         const LightSample ls = light_sample(sc.sh, L, f.P, f.N, rng.u(vertex_dim(vtx, kDimLightSample)),
                                                             rng.u(vertex_dim(vtx, kDimLightSample + 1)));
                         float cost = dot(f.N, ls.dir);
