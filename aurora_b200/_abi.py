@@ -27,6 +27,7 @@ STATUS_NAMES = {0: "AUR_OK", 1: "AUR_ERR_INVALID_ARG", 2: "AUR_ERR_OOM", 3: "AUR
 
 MAT_MATTE, MAT_KELEMEN, MAT_COOKTORRANCE, MAT_METAL, MAT_CONSTANT, MAT_GLASS = 0, 1, 2, 3, 4, 5
 LIGHT_SQUARE, LIGHT_SPHERE, LIGHT_ENV = 0, 1, 2
+NORMAL_NONE, NORMAL_TEXTURE, NORMAL_CONSTANT = 0, 1, 2
 ERR_INVALID_ARG, ERR_OOM, ERR_CUDA, ERR_TIMEOUT, ERR_QUEUE_OVERFLOW, ERR_PARSE, ERR_IO, ERR_UNSUPPORTED = range(1, 9)
 FILM_PFM, FILM_EXR_HALF, FILM_EXR_FLOAT = 0, 1, 2
 RENDER_PLAIN, RENDER_WAVEFRONT = 0, 1
@@ -51,7 +52,7 @@ class MaterialDesc(C.Structure):
     _fields_ = [("type", C.c_int32), ("diffuse", f3), ("specular", f3), ("gain", f3), ("roughness", C.c_float),
                 ("roughness_b", C.c_float), ("reflectance", C.c_float), ("mix", C.c_float),
                 ("diffuse_tex", C.c_int32), ("specular_tex", C.c_int32), ("roughness_tex", C.c_int32),
-                ("ior", C.c_float)]
+                ("ior", C.c_float), ("normal_kind", C.c_int32), ("normal_tex", C.c_int32), ("normal", f3)]
 
 
 class LightDesc(C.Structure):
@@ -66,7 +67,8 @@ class SceneDesc(C.Structure):
                 ("attr_material", C.c_void_p), ("attr_emission", C.c_void_p), ("nattr", C.c_uint32),
                 ("materials", C.c_void_p), ("nmat", C.c_uint32), ("lights", C.c_void_p), ("nlight", C.c_uint32),
                 ("texels", C.c_void_p), ("tex_dims", C.c_void_p), ("ntex", C.c_uint32), ("fov", C.c_float),
-                ("width", C.c_int32), ("height", C.c_int32)]
+                ("width", C.c_int32), ("height", C.c_int32), ("tex_triplanar_scale", C.c_void_p),
+                ("attr_camera_to_object", C.c_void_p)]
 
 
 class RenderOpts(C.Structure):

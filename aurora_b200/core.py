@@ -57,7 +57,7 @@ class Context:
     def probe(self, kind: int, records: np.ndarray, scene: "Scene | None" = None) -> np.ndarray:
         records = np.ascontiguousarray(records, np.float32)
         n = records.shape[0]
-        out_w = [7, 3, 1, 1, 3, 1, 8, 2, 1, 5][kind]
+        out_w = [7, 3, 1, 1, 3, 1, 8, 2, 1, 5, 11][kind]
         out = np.zeros((n, out_w), np.float32)
         check(lib().aur_shading_probe(self.handle, scene.handle if scene else None, kind, _ptr(records), n,
                                       _ptr(out)), "aur_shading_probe")

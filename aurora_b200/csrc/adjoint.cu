@@ -240,28 +240,31 @@ __device__ __forceinline__ float kelemen_score(const ShadeScene& sh, const Mater
 
 // Which parameter a vertex's lobe depends on.
 struct ParamRef {
-    int kind;        // 0 none, 1 diffuse colour of material `index`, 2 texel block `index` (3 floats), 3 roughness
+    int kind;        // 0 none, 1 diffuse colour of material `index`, 2 texels `taps`, 3 roughness
     int index;
     float dr;        // roughness: d r_eff / d r (caustic blur on matte paths)
+    Taps taps;       // kind 2: texel blocks (3 floats each, index from the texel array start) and
+                     // the weights the shader blends them with (1 for the uv lookup; 0 = unused)
 };
 
 __device__ __forceinline__ ParamRef param_of(const ShadeScene& sh, int mat_id, const Brdf& b, const Frame& f,
                                              bool matte, float lobe_u) {
-    ParamRef p{0, 0, 0.f};
+    ParamRef p;
+    p.kind = 0; p.index = 0; p.dr = 0.f;
+    for (int k = 0; k < 3; ++k) { p.taps.idx[k] = 0; p.taps.w[k] = 0.f; }
     const Material m = sh.mats[mat_id];
     if (b.lobe == LOBE_MATTE) {
         if (m.type != MAT_MATTE && m.type != MAT_KELEMEN) return p;
         if (m.diff_tex >= 0) {
             const Texture t = sh.texs[m.diff_tex];
-            const float fs = f.su - (float)aur_floor(f.su);
-            const float ft = 1.f - (f.sv - (float)aur_floor(f.sv));
-            int x = aur_floor(fs * (float)t.w), y = aur_floor(ft * (float)t.h);
-            if (y == t.h) y -= 1;
-            if (x == t.w) x -= 1;
-            x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
-            y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
             p.kind = 2;
-            p.index = (t.offset / 3) + y * t.w + x;
+            if (t.tri_scale == 0.f) {
+                p.taps.idx[0] = uv_texel_index(t, f.su, f.sv);
+                p.taps.w[0] = 1.f;
+            } else {
+                p.taps = triplanar_taps(sh.attr_c2o + (size_t)f.attr * 16, t, f.P, f.Ng, false);
+            }
+            for (int k = 0; k < 3; ++k) p.taps.idx[k] += t.offset / 3;
         } else {
             p.kind = 1;
             p.index = mat_id;
@@ -307,7 +310,7 @@ __device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams
         if (kind == RAY_DIFFUSE) matte = true;
         if (collects_emission(kind)) collected += T * at.emission;
         const float lobe_u = rng.u(vertex_dim(vtx, kDimLobe));
-        const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte, lobe_u);
+        const Brdf brdf = get_brdf(sc.sh, at.material, f, matte, lobe_u);
         const ParamRef pr = param_of(sc.sh, at.material, brdf, f, matte, lobe_u);
         float3 dD;
         const float3 D = direct<false, true>(sc, f, brdf, rng, vtx, rc, &vis, &dD);
@@ -343,9 +346,15 @@ __device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams
             if (pr.kind == 1) {
                 mc.add3(pr.index, g, s_g, s_c);
             } else {
-                comp_add(&g_tex[3 * pr.index + 0], &g_tex_c[3 * pr.index + 0], g.x);
-                comp_add(&g_tex[3 * pr.index + 1], &g_tex_c[3 * pr.index + 1], g.y);
-                comp_add(&g_tex[3 * pr.index + 2], &g_tex_c[3 * pr.index + 2], g.z);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const int i = pr.taps.idx[k];
+                    const float wk = pr.taps.w[k];
+                    if (!(wk > 0.f)) continue;
+                    comp_add(&g_tex[3 * i + 0], &g_tex_c[3 * i + 0], g.x * wk);
+                    comp_add(&g_tex[3 * i + 1], &g_tex_c[3 * i + 1], g.y * wk);
+                    comp_add(&g_tex[3 * i + 2], &g_tex_c[3 * i + 2], g.z * wk);
+                }
             }
         } else if (pr.kind == 3) {
             const float3 g = dp * (gdir * pr.dr + gcont * pr.dr);
@@ -408,7 +417,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         const Attr at = sc.sh.attrs[f.attr];
                         if (kind == RAY_DIFFUSE) matte = true;
                         if (collects_emission(kind)) Lo += T * at.emission;
-                        const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
+                        const Brdf brdf = get_brdf(sc.sh, at.material, f, matte,
                                                    rng.u(vertex_dim(vtx, kDimLobe)));
                         uint32_t vis = 0;
                         Lo += direct<true, false>(sc, f, brdf, rng, vtx, rc, &vis, nullptr) * T;

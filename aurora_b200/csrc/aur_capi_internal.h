@@ -42,6 +42,7 @@ struct aur_scene {
     aur::Light* lights = nullptr;
     aur::Texture* texs = nullptr;
     float* texels = nullptr;
+    float* attr_c2o = nullptr;                 // 16 floats per attribute
     // host copies
     std::vector<aur::Material> h_mats;
     std::vector<aur::Light> h_lights;

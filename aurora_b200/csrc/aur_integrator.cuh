@@ -163,7 +163,7 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         const Attr at = sc.sh.attrs[f.attr];
         if (kind == RAY_DIFFUSE) matte_path = true;
         if (collects_emission(kind)) Lo += T * at.emission;
-        const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte_path,
+        const Brdf brdf = get_brdf(sc.sh, at.material, f, matte_path,
                                    rng.u(vertex_dim(vtx, kDimLobe)));
         Lo += integrate_direct(sc, f, brdf, rng, vtx, rc) * T;
         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),

@@ -14,6 +14,8 @@
 //   square light              Aurora/src/lights/squareLight.h:57-122, squareLight.cpp:20-52
 //   triangle test             Aurora/src/geometry/renderableTriangle.cpp:33-123
 //   texture2D (nearest)       Aurora/src/shading/shaders/texture2DShader.h:28-31, frontend/texture2D.cpp:48-72
+//   triplanar texture         Aurora/src/shading/shaders/triplanarTextureShader.h:29-51 (colour), :71-93 (float)
+//   normal map                Aurora/src/shading/materials/material.cpp:27-40, frontend/integrator.cpp:132-150
 // The sphere light has no reference counterpart (uniform cone sampling of the
 // subtended solid angle, as in Shirley & Wang 1994 / pbrt v3 section 14.2).
 #pragma once
@@ -29,7 +31,7 @@ enum MatType : int { MAT_MATTE = 0, MAT_KELEMEN = 1, MAT_COOKTORRANCE = 2, MAT_M
 enum LobeType : int { LOBE_MATTE = 0, LOBE_SPEC = 1, LOBE_MIRROR = 2, LOBE_CONSTANT = 3, LOBE_TRANSMIT = 4 };
 enum LightType : int { LIGHT_SQUARE = 0, LIGHT_SPHERE = 1, LIGHT_ENV = 2 };
 
-struct Material {            // 80 B
+struct Material {            // 96 B
     int type;
     int diff_tex, spec_tex, rough_tex;   // texture index or -1
     float3 diff;             // matte colour / Kelemen diffusecolor
@@ -40,7 +42,10 @@ struct Material {            // 80 B
     float mix;               // metal mix
     int table;               // Kelemen albedo table index (64x32 floats each)
     float ior;               // glass index of refraction
+    int norm_tex;            // normal-map shader: texture index, kNormalNone or kNormalConst
+    float3 norm;             // kNormalConst: the constant tangent-space map colour
 };
+constexpr int kNormalNone = -1, kNormalConst = -2;
 struct Attr {                // AttributeState: material + emission (attributeState.h)
     int material;
     float3 emission;
@@ -59,7 +64,9 @@ struct Light {
     float pdf_norm;          // env: mean texel luminance (Texture2D::initPdf)
     int pad;
 };
-struct Texture { int w, h, offset, pad; };   // texels: RGB float, offset in floats
+// A texture shader over one image (texels: RGB float, offset in floats): tri_scale 0 is
+// the uv lookup (texture2DShader), > 0 the triplanar projection with that scale.
+struct Texture { int w, h, offset; float tri_scale; };
 struct Camera { float fov; int w, h; int pad; };
 
 struct ShadeScene {          // device pointers for the shading stage
@@ -74,7 +81,14 @@ struct ShadeScene {          // device pointers for the shading stage
     const float* corner_uv;  // per-corner uvs, 6 floats per triangle
     const int* tri_attr;     // attribute index per triangle
     int nlights;
+    int nnormal;             // materials with a normal map
+    const float* attr_c2o;   // camera-to-object transform per attribute, 16 floats row major
 };
+
+// Shading point at a hit (ShadingGeometry + Integrator::LocalGeometry): P the hit point,
+// Ng the interpolated face-forwarded normal, N the shading normal (normal map, then the
+// back-facing fix), V = -normalize(dir), (su, sv) the interpolated uv.
+struct Frame { float3 P, V, N, Ng; float su, sv; int attr; };
 
 struct RayF { float3 o; float mint; float3 d; float maxt; };
 
@@ -138,8 +152,8 @@ AUR_HD bool tri_intersect(float3 p1, float3 e1, float3 e2, float3 o, float3 d, f
 
 // ------------------------------------------------------------------ textures
 AUR_HD int aur_floor(float x) { return (int)x - (x < 0.f && (float)(int)x != x); }   // math_utils.h floor
-AUR_HD float3 tex_read(const ShadeScene& s, int tex, float su, float sv) {
-    Texture t = s.texs[tex];
+// texel of the uv lookup (texture2DShader: wrap to [0, 1), flip t)
+AUR_HD int uv_texel_index(const Texture& t, float su, float sv) {
     float fs = su - (float)aur_floor(su);
     float ft = 1.f - (sv - (float)aur_floor(sv));
     int x = aur_floor(fs * (float)t.w);
@@ -148,8 +162,104 @@ AUR_HD float3 tex_read(const ShadeScene& s, int tex, float su, float sv) {
     if (x == t.w) x -= 1;
     x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
     y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
-    const float* p = s.texels + t.offset + 3 * (y * t.w + x);
+    return y * t.w + x;
+}
+// Texture2D::read / ::pdf with filter 0 at (s, t) (texture2D.cpp:48-72, 112-134): the texel
+// floor(s w), floor(t h), no wrap and no flip (unlike the uv shader lookup)
+AUR_HD int texel_index(const Texture& t, float s, float v) {
+    int x = (int)floorf(s * (float)t.w), y = (int)floorf(v * (float)t.h);
+    if (y == t.h) y -= 1;
+    if (x == t.w) x -= 1;
+    x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
+    y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
+    return y * t.w + x;
+}
+AUR_HD float3 texel_rgb(const ShadeScene& s, const Texture& t, int i) {
+    const float* p = s.texels + t.offset + 3 * i;
     return mk(p[0], p[1], p[2]);
+}
+
+// The texels a triplanar shader blends and their weights (triplanarTextureShader.h):
+// the colour shader weighs the axes by |N_obj| - 0.25 of the object-space normal, the
+// float shader by |Ng| - 0.2 of the camera-space normal; the texture is read at
+// (|fmod(P_obj[i+1] / scale, 1)|, |fmod(P_obj[i+2] / scale, 1)|) for each axis i of
+// positive weight. Tap i (axis i) is texel idx[i] with weight w[i]; w[i] = 0 skips it.
+struct Taps { int idx[3]; float w[3]; };
+AUR_HD Taps triplanar_taps(const float* c2o, const Texture& t, float3 P, float3 Ng, bool float_shader) {
+    const float* m = c2o;
+    float w[3];
+    float3 N;
+    double cut;
+    if (float_shader) {
+        N = Ng;
+        cut = 0.2;
+    } else {                                           // (*cameraToObject)(Ng), a vector
+        N = normalize(mk(m[0] * Ng.x + m[1] * Ng.y + m[2] * Ng.z, m[4] * Ng.x + m[5] * Ng.y + m[6] * Ng.z,
+                         m[8] * Ng.x + m[9] * Ng.y + m[10] * Ng.z));
+        cut = 0.25;
+    }
+    const float n3[3] = {N.x, N.y, N.z};
+    float sum = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        float a = fabsf(n3[i]);
+        a = (float)((double)a - cut);                  // weights[i] -= 0.25 (0.2): a double constant
+        a = a > 0.f ? a : 0.f;                         // max(weights[i], 0.f)
+        w[i] = a;
+        sum = sum + a;
+    }
+#pragma unroll
+    for (int i = 0; i < 3; ++i) w[i] = w[i] / sum;
+    // (*cameraToObject)(P), a point (transform.cpp:206-214), then P /= scale
+    float x = m[0] * P.x + m[1] * P.y + m[2] * P.z + m[3];
+    float y = m[4] * P.x + m[5] * P.y + m[6] * P.z + m[7];
+    float z = m[8] * P.x + m[9] * P.y + m[10] * P.z + m[11];
+    const float wp = m[12] * P.x + m[13] * P.y + m[14] * P.z + m[15];
+    if (wp != 1.f) {
+        const float iw = 1.f / wp;
+        x = x * iw; y = y * iw; z = z * iw;
+    }
+    const float inv = 1.f / t.tri_scale;
+    const float p3[3] = {x * inv, y * inv, z * inv};
+    Taps r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        r.idx[i] = 0;
+        r.w[i] = w[i] > 0.f ? w[i] : 0.f;              // if (weights[i] > 0): NaN weights skip too
+        if (!(w[i] > 0.f)) continue;
+        const float ss = fabsf(fmodf(p3[(i + 1) % 3], 1.f));
+        const float tt = fabsf(fmodf(p3[(i + 2) % 3], 1.f));
+        r.idx[i] = texel_index(t, ss, tt);
+    }
+    return r;
+}
+// The triplanar shaders' value (out of line: rare, and its arrays stay out of the callers'
+// frames); `rgb` selects the colour shader, else the float shader's red channel in .x.
+static __host__ __device__ __noinline__ float3 triplanar_eval(const float* texels, Texture t, const float* c2o, float3 P,
+                                                              float3 Ng, bool rgb) {
+    const Taps k = triplanar_taps(c2o, t, P, Ng, !rgb);
+    float3 r = mk(0.f, 0.f, 0.f);
+    float rf = 0.f;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        if (!(k.w[i] > 0.f)) continue;
+        const float* p = texels + t.offset + 3 * k.idx[i];
+        if (rgb) r = r + mk(p[0], p[1], p[2]) * k.w[i];
+        else rf = rf + p[0] * k.w[i];
+    }
+    return rgb ? r : mk(rf, 0.f, 0.f);
+}
+// Shader<Color>::evaluate of a texture shader at a shading point
+AUR_HD float3 shader_color(const ShadeScene& s, int tex, const Frame& f) {
+    const Texture t = s.texs[tex];
+    if (t.tri_scale == 0.f) return texel_rgb(s, t, uv_texel_index(t, f.su, f.sv));
+    return triplanar_eval(s.texels, t, s.attr_c2o + (size_t)f.attr * 16, f.P, f.Ng, true);
+}
+// Shader<float>::evaluate: the red channel
+AUR_HD float shader_float(const ShadeScene& s, int tex, const Frame& f) {
+    const Texture t = s.texs[tex];
+    if (t.tri_scale == 0.f) return s.texels[t.offset + 3 * uv_texel_index(t, f.su, f.sv)];
+    return triplanar_eval(s.texels, t, s.attr_c2o + (size_t)f.attr * 16, f.P, f.Ng, false).x;
 }
 
 // ------------------------------------------------------------------ BRDF lobes
@@ -301,23 +411,23 @@ AUR_HD float kelemen_albedo(const float* table, float costheta, float roughness)
 // roughness * (1 - CAUSTIC_BLUR) + CAUSTIC_BLUR with the reference's double constants
 AUR_HD float caustic_blur(float r) { return (float)((double)r * (1.0 - 0.2) + 0.2); }
 
-// Material::getBrdf for every supported material. `lobe_u` is the vertex's
-// lobe-choice random number; `st` the interpolated uv.
-AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float su, float sv,
-                     bool matte_path, float lobe_u) {
+// Material::getBrdf for every supported material at shading point `f`. `lobe_u` is the
+// vertex's lobe-choice random number.
+AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, const Frame& f, bool matte_path, float lobe_u) {
+    const float3 V = f.V, N = f.N;
     Material m = s.mats[mat_id];
     Brdf b;
     if (m.type == MAT_MATTE) {
         b.lobe = LOBE_MATTE;
-        b.color = m.diff_tex >= 0 ? tex_read(s, m.diff_tex, su, sv) : m.diff;
+        b.color = m.diff_tex >= 0 ? shader_color(s, m.diff_tex, f) : m.diff;
         b.rough = 0.f;
         return b;
     }
     if (m.type == MAT_KELEMEN || m.type == MAT_COOKTORRANCE) {
-        float rough = m.rough_tex >= 0 ? tex_read(s, m.rough_tex, su, sv).x : m.rough;
+        float rough = m.rough_tex >= 0 ? shader_float(s, m.rough_tex, f) : m.rough;
         if (matte_path) rough = caustic_blur(rough);
         b.lobe = LOBE_SPEC;
-        b.color = m.spec_tex >= 0 ? tex_read(s, m.spec_tex, su, sv) : m.spec;
+        b.color = m.spec_tex >= 0 ? shader_color(s, m.spec_tex, f) : m.spec;
         b.rough = rough;
         if (m.type == MAT_KELEMEN && m.refl < 1.f) {
             float c = dot(N, V);
@@ -325,7 +435,7 @@ AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, float3 V, float3 N, float 
             float albedo = kelemen_albedo(s.albedo + (size_t)m.table * (kAlbedoCos * kAlbedoRough), c, rough);
             if (lobe_u > albedo) {
                 b.lobe = LOBE_MATTE;
-                b.color = m.diff_tex >= 0 ? tex_read(s, m.diff_tex, su, sv) : m.diff;
+                b.color = m.diff_tex >= 0 ? shader_color(s, m.diff_tex, f) : m.diff;
                 b.rough = 0.f;
             }
         }
@@ -370,19 +480,9 @@ AUR_HD float3 xform_vector(const float* m, float3 v) {                  // trans
     return mk(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
               m[8] * v.x + m[9] * v.y + m[10] * v.z);
 }
-// Texture2D::read / ::pdf with filter 0 at (s, t) (texture2D.cpp:48-72, 112-134): the texel
-// floor(s w), floor(t h), no wrap and no flip (unlike the uv shader lookup)
-AUR_HD int env_texel_index(const Texture& t, float s, float v) {
-    int x = (int)floorf(s * (float)t.w), y = (int)floorf(v * (float)t.h);
-    if (y == t.h) y -= 1;
-    if (x == t.w) x -= 1;
-    x = x < 0 ? 0 : (x > t.w - 1 ? t.w - 1 : x);
-    y = y < 0 ? 0 : (y > t.h - 1 ? t.h - 1 : y);
-    return y * t.w + x;
-}
 AUR_HD float3 env_texel(const ShadeScene& sh, int tex, float s, float v) {
     const Texture t = sh.texs[tex];
-    const float* p = sh.texels + t.offset + 3 * env_texel_index(t, s, v);
+    const float* p = sh.texels + t.offset + 3 * texel_index(t, s, v);
     return mk(p[0], p[1], p[2]);
 }
 // the map's pdf: texel luminance (r + g + b) / 3 over its mean (Texture2D::initPdf)
@@ -577,9 +677,32 @@ AUR_HD float light_pdf(const ShadeScene& sh, const Light& l, float3 o, float3 d,
 
 AUR_HD float power_heuristic(float f, float g) { return (f * f) / (f * f + g * g); }  // integrator.cpp:28-31
 
+// Material::runNormalShader (material.cpp:27-40): the map colour read as a tangent-space
+// vector around Ng (tangentToWorld), normalised unless zero; out of line, as only scenes
+// with normal maps take it (arguments by value or global pointer, so that nothing of the
+// caller's moves to local memory).
+static __host__ __device__ __noinline__ float3 normal_map(const Material* mats, const Texture* texs, const float* texels,
+                                                          const float* attr_c2o, int mat, float3 P, float3 Ng,
+                                                          float su, float sv, int attr) {
+    const Material& m = mats[mat];
+    float3 c = m.norm;
+    if (m.norm_tex != kNormalConst) {
+        ShadeScene s;
+        s.texs = texs;
+        s.texels = texels;
+        s.attr_c2o = attr_c2o;
+        Frame f;
+        f.P = P; f.Ng = Ng; f.su = su; f.sv = sv; f.attr = attr;
+        c = shader_color(s, m.norm_tex, f);
+    }
+    const float3 ns = tangent_to_world(c, Ng);
+    if (!(ns.x != 0.f || ns.y != 0.f || ns.z != 0.f)) return Ng;
+    return normalize(ns);
+}
+
 // Shading frame at a hit (embreeAccelerator.cpp:54-90 + integrator.cpp:132-150):
-// interpolated, face-forwarded, normalised normal; V = -normalize(dir); back-facing fix.
-struct Frame { float3 P, V, N; float su, sv; int attr; };
+// interpolated, face-forwarded, normalised normal; the normal map; V = -normalize(dir);
+// back-facing fix.
 AUR_HD Frame hit_frame(const ShadeScene& s, int prim, float t, float u, float v, float3 o, float3 d, bool need_uv) {
     Frame f;
     const float* n = s.corner_n + (size_t)prim * 9;
@@ -588,7 +711,8 @@ AUR_HD Frame hit_frame(const ShadeScene& s, int prim, float t, float u, float v,
                    w * n[1] + u * n[4] + v * n[7],
                    w * n[2] + u * n[5] + v * n[8]);
     if (dot(nn, d) > 0.f) nn *= -1.f;
-    f.N = normalize(nn);
+    f.Ng = normalize(nn);
+    f.N = f.Ng;
     f.P = o + d * t;
     f.attr = s.tri_attr[prim];
     f.su = f.sv = 0.f;
@@ -596,6 +720,11 @@ AUR_HD Frame hit_frame(const ShadeScene& s, int prim, float t, float u, float v,
         const float* uv = s.corner_uv + (size_t)prim * 6;
         f.su = w * uv[0] + u * uv[2] + v * uv[4];
         f.sv = w * uv[1] + u * uv[3] + v * uv[5];
+    }
+    if (s.nnormal) {
+        const int mat = s.attrs[f.attr].material;
+        if (s.mats[mat].norm_tex != kNormalNone)
+            f.N = normal_map(s.mats, s.texs, s.texels, s.attr_c2o, mat, f.P, f.Ng, f.su, f.sv, f.attr);
     }
     f.V = -normalize(d);
     if (dot(f.V, f.N) <= 0.f) {

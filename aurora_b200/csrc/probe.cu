@@ -8,10 +8,11 @@ using namespace aur;
 
 namespace {
 
-constexpr int kInH[10] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11};
-constexpr int kOutH[10] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5};
-__constant__ int kIn[10] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11};
-__constant__ int kOut[10] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5};
+constexpr int kKinds = 11;
+constexpr int kInH[kKinds] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11, 12};
+constexpr int kOutH[kKinds] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5, 11};
+__constant__ int kIn[kKinds] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11, 12};
+__constant__ int kOut[kKinds] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5, 11};
 
 __global__ void k_probe(int kind, const float* in, uint32_t n, float* out, ShadeScene sh, const float* tables) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -50,9 +51,20 @@ __global__ void k_probe(int kind, const float* in, uint32_t n, float* out, Shade
         o[1] = maxt;
     } else if (kind == 8) {
         o[0] = light_visible(sh.lights[(int)q[0]], mk(q[1], q[2], q[3]), mk(q[4], q[5], q[6])) ? 1.f : 0.f;
-    } else {
-        Brdf b = get_brdf(sh, (int)q[0], mk(q[1], q[2], q[3]), mk(q[4], q[5], q[6]), q[7], q[8], q[9] != 0.f, q[10]);
+    } else if (kind == 9) {
+        Frame f;
+        f.P = mk(0.f, 0.f, 0.f);
+        f.V = mk(q[1], q[2], q[3]);
+        f.N = f.Ng = mk(q[4], q[5], q[6]);
+        f.su = q[7]; f.sv = q[8];
+        f.attr = 0;
+        Brdf b = get_brdf(sh, (int)q[0], f, q[9] != 0.f, q[10]);
         o[0] = (float)b.lobe; o[1] = b.color.x; o[2] = b.color.y; o[3] = b.color.z; o[4] = b.rough;
+    } else {
+        const Frame f = hit_frame(sh, (int)q[0], q[1], q[2], q[3], mk(q[4], q[5], q[6]), mk(q[7], q[8], q[9]), true);
+        Brdf b = get_brdf(sh, sh.attrs[f.attr].material, f, q[10] != 0.f, q[11]);
+        o[0] = f.N.x; o[1] = f.N.y; o[2] = f.N.z; o[3] = f.Ng.x; o[4] = f.Ng.y; o[5] = f.Ng.z;
+        o[6] = (float)b.lobe; o[7] = b.color.x; o[8] = b.color.y; o[9] = b.color.z; o[10] = b.rough;
     }
 }
 
@@ -61,7 +73,7 @@ __global__ void k_probe(int kind, const float* in, uint32_t n, float* out, Shade
 extern "C" aur_status aur_shading_probe(aur_ctx* ctx, aur_scene* scene, int kind, const float* in, uint32_t n,
                                         float* out) {
     if (!ctx || (n && (!in || !out))) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: NULL argument");
-    if (kind < 0 || kind > 9) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: unknown kind");
+    if (kind < 0 || kind >= kKinds) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: unknown kind");
     if (kind >= 6 && !scene) return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: this kind needs a scene");
     if (n == 0) return AUR_OK;
     DeviceGuard g(ctx->device);
@@ -82,6 +94,8 @@ extern "C" aur_status aur_shading_probe(aur_ctx* ctx, aur_scene* scene, int kind
             return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: bad light index");
         if (kind == 9 && (idx < 0.f || idx >= (float)scene->h_mats.size()))
             return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: bad material index");
+        if (kind == 10 && (idx < 0.f || idx >= (float)scene->ntri))
+            return fail(AUR_ERR_INVALID_ARG, "aur_shading_probe: bad triangle index");
     }
     DevIn di;
     DevOut dout;

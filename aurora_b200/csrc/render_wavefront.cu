@@ -409,7 +409,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 const Attr at = sc.sh.attrs[f.attr];
                 if (kind == RAY_DIFFUSE) matte = true;
                 if (collects_emission(kind)) Lo += T * at.emission;
-                const Brdf brdf = get_brdf(sc.sh, at.material, f.V, f.N, f.su, f.sv, matte,
+                const Brdf brdf = get_brdf(sc.sh, at.material, f, matte,
                                            rng.u(vertex_dim(vtx, kDimLobe)));
                 // next-event estimation: rays and their unoccluded contributions
                 if (brdf.lobe == LOBE_MATTE || brdf.lobe == LOBE_SPEC) {

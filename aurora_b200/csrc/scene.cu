@@ -87,6 +87,9 @@ static Material make_material(const aur_material_desc& d) {
     m.mix = d.mix;
     m.ior = d.ior;
     m.table = d.type == AUR_MAT_KELEMEN ? kelemen_index(d.reflectance) : 0;
+    m.norm_tex = d.normal_kind == AUR_NORMAL_TEXTURE ? d.normal_tex
+               : d.normal_kind == AUR_NORMAL_CONSTANT ? kNormalConst : kNormalNone;
+    m.norm = mk(d.normal[0], d.normal[1], d.normal[2]);
     return m;
 }
 
@@ -106,7 +109,8 @@ static void scene_free(aur_scene* sc) {
     cudaStreamSynchronize(s);
     bvh_free_device(&sc->bvh.bvh, s);
     cudaStreamSynchronize(s);
-    void* bufs[] = {sc->bvh.tri_attr, sc->corner_n, sc->corner_uv, sc->attrs, sc->mats, sc->lights, sc->texs, sc->texels};
+    void* bufs[] = {sc->bvh.tri_attr, sc->corner_n, sc->corner_uv, sc->attrs, sc->mats, sc->lights, sc->texs, sc->texels,
+                    sc->attr_c2o};
     for (void* b : bufs) if (b) cudaFree(b);
     delete sc;
 }
@@ -129,6 +133,9 @@ DevScene aur_scene::dev() const {
     d.sh.nlights = (int)h_lights.size();
     d.sh.nenv = 0;
     for (const Light& l : h_lights) d.sh.nenv += l.type == LIGHT_ENV ? 1 : 0;
+    d.sh.nnormal = 0;
+    for (const Material& m : h_mats) d.sh.nnormal += m.norm_tex != kNormalNone ? 1 : 0;
+    d.sh.attr_c2o = attr_c2o;
     d.cam = cam;
     return d;
 }
@@ -161,7 +168,16 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     for (uint32_t t = 0; t < d->ntex; ++t) {
         const int w = d->tex_dims[2 * t], h = d->tex_dims[2 * t + 1];
         if (w <= 0 || h <= 0) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: bad texture size");
-        texs[t].w = w; texs[t].h = h; texs[t].offset = (int)texel_floats; texs[t].pad = 0;
+        texs[t].w = w; texs[t].h = h; texs[t].offset = (int)texel_floats;
+        texs[t].tri_scale = 0.f;
+        if (d->tex_triplanar_scale) {
+            if (is_device_ptr(d->tex_triplanar_scale))
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: triplanar scales must be host memory");
+            const float sc = d->tex_triplanar_scale[t];
+            if (!(sc >= 0.f) || !std::isfinite(sc))
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: triplanar scale must be finite and >= 0");
+            texs[t].tri_scale = sc;
+        }
         texel_floats += 3u * (uint32_t)w * (uint32_t)h;
     }
     std::vector<Material> mats(d->nmat);
@@ -174,6 +190,10 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
         const int tx[3] = {md.diffuse_tex, md.specular_tex, md.roughness_tex};
         for (int k = 0; k < 3; ++k)
             if (tx[k] >= (int)d->ntex || tx[k] < -1) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: texture index");
+        if (md.normal_kind < AUR_NORMAL_NONE || md.normal_kind > AUR_NORMAL_CONSTANT)
+            return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: unknown normal-map kind");
+        if (md.normal_kind == AUR_NORMAL_TEXTURE && (md.normal_tex < 0 || md.normal_tex >= (int)d->ntex))
+            return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: normal-map texture index");
         mats[m] = make_material(md);
     }
     std::vector<Light> lights(d->nlight);
@@ -189,6 +209,8 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
                 return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: environment texture index");
             if (ld.tex >= 0 && is_device_ptr(d->texels))
                 return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: an env map needs host texels");
+            if (ld.tex >= 0 && texs[ld.tex].tri_scale != 0.f)
+                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: an env map must be a plain (uv) texture");
         }
         lights[l] = make_light(ld, texs, d->texels);
     }
@@ -220,6 +242,14 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
         cudaMemcpy(ae.data(), d->attr_emission, sizeof(float) * 3 * d->nattr, cudaMemcpyDefault);
         for (uint32_t i = 0; i < d->nattr; ++i) { attrs[i].material = am[i]; attrs[i].emission = mk(ae[3 * i], ae[3 * i + 1], ae[3 * i + 2]); }
     }
+    // cameraToObject per attribute (identity when not given)
+    std::vector<float> c2o(16 * (size_t)d->nattr, 0.f);
+    if (d->attr_camera_to_object) {
+        cudaMemcpy(c2o.data(), d->attr_camera_to_object, sizeof(float) * c2o.size(), cudaMemcpyDefault);
+    } else {
+        for (uint32_t i = 0; i < d->nattr; ++i)
+            for (int k = 0; k < 4; ++k) c2o[16 * (size_t)i + 5 * k] = 1.f;
+    }
     cudaError_t e = cudaSuccess;
     for (const Material& m : mats)
         if (m.type == MAT_KELEMEN && e == cudaSuccess) e = ctx_kelemen_ensure(ctx, m.table);
@@ -230,6 +260,7 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     if (e == cudaSuccess) e = upload(&sc->lights, lights.data(), lights.size(), s);
     if (e == cudaSuccess) e = upload(&sc->texs, texs.data(), texs.size(), s);
     if (e == cudaSuccess) e = upload(&sc->texels, d->texels, texel_floats, s);
+    if (e == cudaSuccess) e = upload(&sc->attr_c2o, c2o.data(), c2o.size(), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { scene_free(sc); return cuda_fail(e, "aur_scene_create"); }
     *out = sc;

@@ -7,8 +7,9 @@
 //
 //   options    resolution, pixelsamples, lightsamples, mindepth, maxdepth, filename
 //   renderCam  fov (slope factor, camera.cpp:51-52), transforms (camera to world)
-//   shaders    texture2DShader (texture files in PFM; EXR needs OpenEXR, not in this build)
-//   materials  matteMaterial, kelemenMaterial, metalMaterial, glassMaterial
+//   shaders    texture2DShader, triplanarTextureShader (texture files in PFM; EXR needs
+//              OpenEXR, not in this build)
+//   materials  matteMaterial, kelemenMaterial, metalMaterial, glassMaterial; normalmap
 //   objects    geometry (OBJ triangles, optional Loop subdivision), light (square), envlight
 //
 // Objects of a JSON object are visited in key order, as the reference's JSON
@@ -32,6 +33,8 @@
 
 struct aur_scene_file {
     std::vector<float> verts, corner_normals, corner_uvs, attr_emission, texels;
+    std::vector<float> tex_scale;   // per texture: 0 = texture2DShader, > 0 = triplanar scale
+    std::vector<float> attr_c2o;    // per attribute: cameraToObject, 16 floats
     std::vector<uint32_t> tri_vidx;
     std::vector<int32_t> tri_attr, attr_material, tex_dims;
     std::vector<aur_material_desc> materials;
@@ -835,8 +838,14 @@ struct Loader {
             const std::string at = need_str(kv.second, "attributetype", where);
             if (at != "color" && at != "float") throw_load(AUR_ERR_PARSE, where + ": unknown attributetype " + at);
             const std::string type = need_str(kv.second, "type", where);
-            if (type != "texture2DShader")
-                throw_load(AUR_ERR_UNSUPPORTED, where + ": shader type " + type + " is not built (texture2DShader is)");
+            float scale = 0.f;
+            if (type == "triplanarTextureShader") {           // jsonParser.cpp:547-551, 568-572
+                scale = (float)need_num(kv.second, "scale", where);
+                if (!(scale > 0.f) || !std::isfinite(scale))
+                    throw_load(AUR_ERR_PARSE, where + ": triplanar scale must be a finite number > 0");
+            } else if (type != "texture2DShader") {
+                throw_load(AUR_ERR_PARSE, where + ": unknown shader type " + type);
+            }
             const std::string path = resolve(dir, need_str(kv.second, "texturename", where));
             const size_t dot = path.find_last_of('.');
             const std::string ext = dot == std::string::npos ? "" : path.substr(dot);
@@ -849,6 +858,7 @@ struct Loader {
             textures[kv.first] = (int)out.tex_dims.size() / 2;
             out.tex_dims.push_back(w);
             out.tex_dims.push_back(h);
+            out.tex_scale.push_back(scale);
             out.texels.insert(out.texels.end(), rgb.begin(), rgb.end());
         }
     }
@@ -861,11 +871,16 @@ struct Loader {
         for (const auto& kv : s->obj) {
             const std::string where = "material \"" + kv.first + "\"";
             const JValue& o = kv.second;
-            if (o.get("normalmap")) throw_load(AUR_ERR_UNSUPPORTED, where + ": normal maps are not built");
             const std::string type = need_str(o, "type", where);
             aur_material_desc m;
             memset(&m, 0, sizeof(m));
             m.diffuse_tex = m.specular_tex = m.roughness_tex = -1;
+            m.normal_kind = AUR_NORMAL_NONE;
+            m.normal_tex = -1;
+            if (o.get("normalmap")) {                        // getMaterial (jsonParser.cpp:317-322)
+                color_attr(o, "normalmap", m.normal, &m.normal_tex, where);
+                m.normal_kind = m.normal_tex >= 0 ? AUR_NORMAL_TEXTURE : AUR_NORMAL_CONSTANT;
+            }
             m.gain[0] = m.gain[1] = m.gain[2] = 1.f;
             m.ior = 1.f;
             if (type == "matteMaterial") {
@@ -898,6 +913,12 @@ struct Loader {
         }
     }
 
+    // AttributeState::cameraToObject of an attribute: the inverse its Transform carries
+    void push_c2o(const Xform& o2c) {
+        for (int i = 0; i < 4; ++i)
+            for (int j = 0; j < 4; ++j) out.attr_c2o.push_back(o2c.inv.m[i][j]);
+    }
+
     void append_mesh(const std::vector<float3>& P, const std::vector<int>& idx, const std::vector<float3>& Ncorner,
                      const std::vector<float2>& UVcorner, int attr) {
         const uint32_t base = (uint32_t)(out.verts.size() / 3);
@@ -927,6 +948,7 @@ struct Loader {
         if (mit == materials.end()) throw_load(AUR_ERR_PARSE, where + ": unknown material \"" + mat + "\"");
         out.attr_material.push_back(mit->second);
         out.attr_emission.insert(out.attr_emission.end(), {0.f, 0.f, 0.f});
+        push_c2o(o2c);
         const Corners cs = read_obj(path);
         std::vector<float3> P, N;
         std::vector<float2> UV;
@@ -982,6 +1004,7 @@ struct Loader {
         append_mesh(P, idx, N, {}, attr);
         const float inten = powf(2.f, l.exposure);
         out.attr_emission.insert(out.attr_emission.end(), {l.color[0] * inten, l.color[1] * inten, l.color[2] * inten});
+        push_c2o(o2c);
     }
 
     // getEnvLight + InfiniteAreaLight (jsonParser.cpp:262-280, infiniteAreaLight.cpp:21-33): the
@@ -1013,10 +1036,12 @@ struct Loader {
             l.tex = (int32_t)(out.tex_dims.size() / 2);
             out.tex_dims.push_back(w);
             out.tex_dims.push_back(h);
+            out.tex_scale.push_back(0.f);
             out.texels.insert(out.texels.end(), rgb.begin(), rgb.end());
         }
         out.lights.push_back(l);
         out.attr_emission.insert(out.attr_emission.end(), {1.f, 1.f, 1.f});   // InfiniteAreaLight::emission()
+        push_c2o(Xform());
         (void)attr;
     }
 
@@ -1077,7 +1102,7 @@ struct Loader {
         aur_material_desc black;
         memset(&black, 0, sizeof(black));
         black.type = AUR_MAT_CONSTANT;
-        black.diffuse_tex = black.specular_tex = black.roughness_tex = -1;
+        black.diffuse_tex = black.specular_tex = black.roughness_tex = black.normal_tex = -1;
         black.gain[0] = black.gain[1] = black.gain[2] = 1.f;
         black.ior = 1.f;
         out.materials.push_back(black);
@@ -1136,6 +1161,8 @@ aur_status aur_scene_file_desc(const aur_scene_file* f, aur_scene_desc* d, aur_r
     d->texels = f->texels.empty() ? nullptr : f->texels.data();
     d->tex_dims = f->tex_dims.empty() ? nullptr : f->tex_dims.data();
     d->ntex = (uint32_t)(f->tex_dims.size() / 2);
+    d->tex_triplanar_scale = f->tex_scale.empty() ? nullptr : f->tex_scale.data();
+    d->attr_camera_to_object = f->attr_c2o.empty() ? nullptr : f->attr_c2o.data();
     d->fov = f->fov;
     d->width = f->width;
     d->height = f->height;

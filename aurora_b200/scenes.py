@@ -156,6 +156,8 @@ class SceneData:
     height: int
     name: str = ""
     render: dict = field(default_factory=dict)   # spp, max_depth, min_depth, seed of the workload
+    tex_triplanar_scale: object = None   # (ntex,) float32: 0 = uv shader, > 0 = triplanar scale; None = all uv
+    attr_c2o: object = None              # (nattr, 16) float32 camera-to-object per attribute; None = identity
     _keep: list = field(default_factory=list, repr=False)
 
     @property
@@ -175,6 +177,14 @@ class SceneData:
         arrs = [np.ascontiguousarray(a) for a in (self.verts, self.tri_vidx, self.tri_attr, self.corner_normals,
                                                   self.corner_uvs, self.attr_material, self.attr_emission)]
         self._keep = [mats, lights, tex, dims] + arrs
+        tscale = None if self.tex_triplanar_scale is None else np.ascontiguousarray(self.tex_triplanar_scale, F32)
+        c2o = None if self.attr_c2o is None else np.ascontiguousarray(self.attr_c2o, F32).reshape(-1, 16)
+        if tscale is not None:
+            assert tscale.shape == (len(self.textures),)
+            self._keep.append(tscale)
+        if c2o is not None:
+            assert c2o.shape[0] == len(self.attr_material)
+            self._keep.append(c2o)
         d = _abi.SceneDesc()
         d.verts, d.nvert = arrs[0].ctypes.data, arrs[0].shape[0]
         d.tri_vidx, d.tri_attr = arrs[1].ctypes.data, arrs[2].ctypes.data
@@ -186,6 +196,8 @@ class SceneData:
         d.tex_dims = dims.ctypes.data if dims.size else None
         d.ntex = len(self.textures)
         d.fov, d.width, d.height = self.fov, self.width, self.height
+        d.tex_triplanar_scale = tscale.ctypes.data if tscale is not None and tscale.size else None
+        d.attr_camera_to_object = c2o.ctypes.data if c2o is not None else None
         return d
 
     def material_params(self) -> np.ndarray:
@@ -195,9 +207,14 @@ class SceneData:
 
 
 def _mat(type_, diffuse=(0, 0, 0), specular=(0, 0, 0), gain=(1, 1, 1), roughness=0.0, roughness_b=0.0,
-         reflectance=0.0, mix=0.0, diffuse_tex=-1, specular_tex=-1, roughness_tex=-1, ior=1.0) -> _abi.MaterialDesc:
+         reflectance=0.0, mix=0.0, diffuse_tex=-1, specular_tex=-1, roughness_tex=-1, ior=1.0, normal_tex=None,
+         normal=None) -> _abi.MaterialDesc:
+    """normal_tex: a texture index used as the normal map; normal: a constant normal-map colour."""
+    kind = (_abi.NORMAL_TEXTURE if normal_tex is not None else
+            _abi.NORMAL_CONSTANT if normal is not None else _abi.NORMAL_NONE)
     return _abi.MaterialDesc(type_, _abi.f3(*diffuse), _abi.f3(*specular), _abi.f3(*gain), roughness, roughness_b,
-                             reflectance, mix, diffuse_tex, specular_tex, roughness_tex, ior)
+                             reflectance, mix, diffuse_tex, specular_tex, roughness_tex, ior, kind,
+                             -1 if normal_tex is None else normal_tex, _abi.f3(*(normal or (0, 0, 0))))
 
 
 def _xform_f32(m: np.ndarray, p: np.ndarray) -> np.ndarray:
@@ -218,15 +235,19 @@ class SceneBuilder:
         self.w2c = np.eye(4) if world_to_camera is None else np.asarray(world_to_camera, np.float64)
         self.materials: list = []
         self.textures: list = []
-        self.objects: list = []     # (verts_cam f32, faces, corner normals f32, corner uvs f32, material)
+        self.tex_scales: list = []  # triplanar scale per texture (0: uv lookup)
+        self.objects: list = []     # (verts_cam f32, faces, corner normals f32, corner uvs f32, material, c2o)
         self.lights: list = []      # (LightDesc, shape verts cam f32, faces, corner normals, emission)
 
     def material(self, type_, **kw) -> int:
         self.materials.append(_mat(type_, **kw))
         return len(self.materials) - 1
 
-    def texture(self, rgb: np.ndarray) -> int:
+    def texture(self, rgb: np.ndarray, triplanar_scale: float = 0.0) -> int:
+        """An image (H, W, 3) as a texture shader: the uv lookup, or with triplanar_scale > 0 the
+        triplanar projection in the object space of the mesh that uses it."""
         self.textures.append(np.ascontiguousarray(rgb, np.float32))
+        self.tex_scales.append(float(triplanar_scale))
         return len(self.textures) - 1
 
     def mesh(self, verts, faces, material, normals=None, uvs=None, object_to_world=None):
@@ -256,7 +277,8 @@ class SceneBuilder:
             cu = np.zeros((faces.shape[0], 6), F32)
         else:
             cu = np.asarray(uvs, np.float64)[faces].astype(F32).reshape(-1, 6)
-        self.objects.append((vc, faces, cn, cu, material))
+        c2o = np.linalg.inv(o2c).astype(F32).ravel()            # AttributeState::cameraToObject
+        self.objects.append((vc, faces, cn, cu, material, c2o))
         return len(self.objects) - 1
 
     def square_light(self, object_to_world, size_x, size_y, color, exposure=0.0):
@@ -315,7 +337,7 @@ class SceneBuilder:
         verts, faces, attr, cn, cu = [], [], [], [], []
         base = 0
         nobj = len(self.objects)
-        for i, (vc, f, n, u, _) in enumerate(self.objects):
+        for i, (vc, f, n, u, _, _) in enumerate(self.objects):
             verts.append(vc); faces.append(f + base); attr.append(np.full(len(f), i, np.int32))
             cn.append(n); cu.append(u); base += len(vc)
         for j, (ld, vc, f, n, em) in enumerate(self.lights):
@@ -325,10 +347,13 @@ class SceneBuilder:
             cn.append(n); cu.append(np.zeros((len(f), 6), F32)); base += len(vc)
         attr_mat = np.array([o[4] for o in self.objects] + [const] * len(self.lights), np.int32)
         attr_em = np.array([[0, 0, 0]] * nobj + [l[4] for l in self.lights], F32).reshape(-1, 3)
+        c2o = np.array([o[5] for o in self.objects] + [np.eye(4, dtype=F32).ravel()] * len(self.lights),
+                       F32).reshape(-1, 16)
+        scales = np.array(self.tex_scales, F32) if any(s != 0.0 for s in self.tex_scales) else None
         return SceneData(np.concatenate(verts).astype(F32), np.concatenate(faces).astype(np.uint32),
                          np.concatenate(attr), np.concatenate(cn).astype(F32), np.concatenate(cu).astype(F32),
                          attr_mat, attr_em, materials, [l[0] for l in self.lights], list(self.textures),
-                         self.fov, self.width, self.height, self.name, dict(render or {}))
+                         self.fov, self.width, self.height, self.name, dict(render or {}), scales, c2o)
 
 
 def load_scene_file(path: str):
@@ -366,11 +391,14 @@ def load_scene_file(path: str):
             n = 3 * int(w_) * int(h_)
             textures.append(texels[off:off + n].reshape(int(h_), int(w_), 3))
             off += n
+        tscale = arr(d.tex_triplanar_scale, d.ntex, np.float32, (d.ntex,)) if d.tex_triplanar_scale else None
+        c2o = arr(d.attr_camera_to_object, 16 * d.nattr, np.float32, (d.nattr, 16)) if d.attr_camera_to_object \
+            else None
         info = {"output": _abi.lib().aur_scene_file_output(h).decode(),
                 "light_samples": int(_abi.lib().aur_scene_file_light_samples(h))}
         data = SceneData(verts, vidx, tattr, cn, cu, amat, aem, mats, lights, textures, float(d.fov), int(d.width),
                          int(d.height), os.path.basename(path),
-                         dict(spp=o.spp, max_depth=o.max_depth, min_depth=o.min_depth, seed=0))
+                         dict(spp=o.spp, max_depth=o.max_depth, min_depth=o.min_depth, seed=0), tscale, c2o)
         return data, o, info
     finally:
         _abi.lib().aur_scene_file_destroy(h)
@@ -451,6 +479,37 @@ def sphere_scene(width=512, height=512, spp=64, max_depth=6, seed=2, ground_text
     b.sphere_light((2.2, 1.2, 1.5), 0.3, (30.0, 24.0, 18.0), 0.0)
     if env is not None:
         b.env_light(**env)
+    return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))
+
+
+def shader_scene(width=128, height=128, spp=16, max_depth=6, seed=3, tex_seed=11, sphere_level=4) -> SceneData:
+    """Texture-shader workload: triplanar colour and roughness shaders, a normal-map texture and a
+    constant normal map. A Kelemen sphere (triplanar diffuse, scale 0.5; triplanar roughness,
+    scale 0.8; constant normal map (0.1, 0.05, 1)) and a rotated Lambert box (triplanar colour,
+    scale 0.3, projected in the box's object space) on a 10x10 Lambert ground (triplanar
+    colour, scale 0.7; a normal-map texture over its uvs), one quad light and one sphere light.
+    Textures uniform random (seed `tex_seed`). Roulette off."""
+    r = np.random.default_rng(tex_seed)
+    b = SceneBuilder(width, height, FOV40, world_to_camera=look_at((0, 1.2, 5.0), (0, 0, 0)), name="shaders")
+    t_ground = b.texture(r.uniform(0.2, 0.8, (32, 32, 3)), triplanar_scale=0.7)
+    nrm = np.concatenate([r.uniform(0.0, 0.3, (16, 16, 2)), r.uniform(0.8, 1.0, (16, 16, 1))], -1)
+    t_nrm = b.texture(nrm)
+    t_sphere = b.texture(r.uniform(0.2, 0.8, (16, 16, 3)), triplanar_scale=0.5)
+    t_rough = b.texture(r.uniform(0.1, 0.6, (8, 8, 3)), triplanar_scale=0.8)
+    t_box = b.texture(r.uniform(0.2, 0.8, (8, 8, 3)), triplanar_scale=0.3)
+    m_ground = b.material(_abi.MAT_MATTE, diffuse=(0.5, 0.5, 0.5), diffuse_tex=t_ground, normal_tex=t_nrm)
+    m_sphere = b.material(_abi.MAT_KELEMEN, diffuse=(0.6, 0.6, 0.6), specular=(1.0, 1.0, 1.0), roughness=0.2,
+                          reflectance=0.5, diffuse_tex=t_sphere, roughness_tex=t_rough, normal=(0.1, 0.05, 1.0))
+    m_box = b.material(_abi.MAT_MATTE, diffuse=(0.5, 0.5, 0.5), diffuse_tex=t_box)
+    gv = np.array([[-5, -1, 5], [5, -1, 5], [5, -1, -5], [-5, -1, -5]], np.float64)
+    guv = np.array([[0, 0], [1, 0], [1, 1], [0, 1]], np.float64) * 4.0
+    b.mesh(gv, np.array([[0, 1, 2], [0, 2, 3]]), m_ground, normals=np.tile([0, 1, 0], (4, 1)), uvs=guv)
+    v, f = icosphere(sphere_level)
+    b.mesh(v, f, m_sphere, normals=v, object_to_world=translate(-0.6, 0.0, 0.0))
+    bv, bf, _ = box_mesh()
+    b.mesh(bv, bf, m_box, object_to_world=translate(1.3, -0.55, 0.6) @ rot_y(35.0) @ scale(0.9, 0.9, 0.9))
+    b.square_light(translate(-2.0, 3.0, 1.0) @ rot_x(-90.0), 0.5, 0.5, (8.0, 8.0, 8.0), 0.0)
+    b.sphere_light((2.2, 1.2, 1.5), 0.3, (30.0, 24.0, 18.0), 0.0)
     return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))
 
 

@@ -133,7 +133,13 @@ typedef struct aur_material_desc {
     int32_t roughness_tex; /* float shader: red channel */
     float ior;             /* glass index of refraction (glass: specular = specColor,
                               diffuse = transmitColor, reflectance = Schlick F0, 1 = mirror) */
+    /* normal map (Material::runNormalShader, Aurora/src/shading/materials/material.cpp:27-40):
+     * the shader's colour, read as a tangent-space vector around the interpolated normal */
+    int32_t normal_kind;   /* AUR_NORMAL_NONE, AUR_NORMAL_TEXTURE or AUR_NORMAL_CONSTANT */
+    int32_t normal_tex;    /* AUR_NORMAL_TEXTURE: texture index */
+    float normal[3];       /* AUR_NORMAL_CONSTANT: the map colour */
 } aur_material_desc;
+enum { AUR_NORMAL_NONE = 0, AUR_NORMAL_TEXTURE = 1, AUR_NORMAL_CONSTANT = 2 };
 
 /* Square light: Aurora/src/lights/squareLight.{h,cpp}; the quad
  * [-size_x,size_x] x [-size_y,size_y] at z=0 mapped by object_to_camera
@@ -177,6 +183,14 @@ typedef struct aur_scene_desc {
     uint32_t ntex;
     float fov;                     /* slope factor, as camera.cpp:51-52 */
     int32_t width, height;
+    /* Texture shaders. Each texture index is one shader over its image: scale 0 is the uv
+     * lookup (texture2DShader, Aurora/src/shading/shaders/texture2DShader.h:28-31), > 0 the
+     * triplanar projection with that scale (triplanarTextureShader.h:29-93). NULL: all uv. */
+    const float* tex_triplanar_scale;   /* ntex */
+    /* AttributeState::cameraToObject per attribute, 16 floats row major (the inverse of
+     * the object's camera-space transform; triplanar shaders project in object space).
+     * NULL: identity for all. */
+    const float* attr_camera_to_object; /* nattr x 16 */
 } aur_scene_desc;
 
 AUR_API aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* desc, const aur_bvh_opts* bvh_opts,
@@ -308,11 +322,16 @@ AUR_API aur_status aur_kelemen_table(aur_ctx* ctx, float reflectance, float* out
  *   3 kelemen       table index, costheta, roughness (3) -> albedo (1)  KelemenMaterial::getAlbedo
  *   4 camera_ray    fov, w, h, px, py, j1, j2 (7) -> dir3 (3)           Camera::convertSample
  *   5 power_heur.   f, g (2) -> weight (1)                              PowerHeuristic
- *   6 light_sample  light, P3, u1, u2 (6) -> dir3, maxt, pdf, color3 (8) Light::generateSample
+ *   6 light_sample  light, P3, u1, u2, N3 (9) -> dir3, maxt, pdf, color3 (8) Light::generateSample
  *   7 light_pdf     light, o3, d3, mint, maxt (9) -> pdf, maxt (2)     Light::pdf
  *   8 light_visible light, P3, N3 (7) -> visible (1)                    Light::visible
  *   9 get_brdf      material, V3, N3, su, sv, matte, lobe_u (11) -> lobe, color3, rough (5)
- * Kinds 6-9 need `scene`. */
+ *                   (shading point at the origin, attribute 0, Ng = N)
+ *  10 shade_point   triangle, t, u, v, o3, d3, matte, lobe_u (12)
+ *                   -> N3, Ng3, lobe, color3, rough (11)
+ *                   the hit's shading frame (interpolated normal, normal map, back-facing
+ *                   fix) and Material::getBrdf there (integrator.cpp:132-150)
+ * Kinds 6-10 need `scene`. */
 AUR_API aur_status aur_shading_probe(aur_ctx* ctx, aur_scene* scene, int kind, const float* in, uint32_t n,
                                      float* out);
 

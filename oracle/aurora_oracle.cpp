@@ -154,6 +154,7 @@ struct Tri { Point p1; Vector e1, e2; };
 struct Mat {
     int type; Color diff, spec, gain; float rough, roughB, refl, mix;
     int diffTex, specTex, roughTex; int table; float ior;
+    int normTex; Color normC;   // normal-map shader: texture, -1 none, -2 the constant colour normC
 };
 struct Light {
     int type; float xScale, yScale, radius; Point pCam[4]; Vector lightN; Color le; Point center; float m[16];
@@ -162,7 +163,8 @@ struct Light {
     // env map texture (or -1), 2^exposure, mean texel luminance
     float minv[16]; int tex; float escale; float pdfNorm;
 };
-struct Tex { int w, h; const float* px; size_t offset; };   // offset: first float in the texel array
+// a texture shader: uv lookup (triScale 0) or triplanar projection with scale triScale
+struct Tex { int w, h; const float* px; size_t offset; float triScale; };   // offset: first float in the texel array
 
 struct BvhNode { float lo[3], hi[3]; int left, right, start, count; };   // leaf if count > 0
 
@@ -176,6 +178,7 @@ struct Scene {
     std::vector<Light> lights;
     std::vector<Tex> texs;
     std::vector<float> texels;
+    std::vector<float> attrC2O;             // AttributeState::cameraToObject, 16 floats per attribute
     const float* albedo = nullptr;          // [table][64][32]
     float fov; int width, height;
     // CPU BVH (binned SAH) used by the timed baseline; brute force when empty
@@ -524,6 +527,10 @@ static float brdfPdf(const BrdfState& b, const Vector& L, const Vector& V, const
     return 0.f;
 }
 
+// ShadingGeometry + Integrator::LocalGeometry at a hit: Ng the interpolated face-forwarded
+// normal, Nn the shading normal (normal map, back-facing fix)
+struct LocalGeometry { Point P; Vector Vn, Nn, Ng; float su, sv; int attr; };
+
 // ------------------------------------------------------------ textures (texture2DShader.h:28-31, texture2D.cpp:48-72)
 static int texelOf(const Tex& t, float u, float v) {     // nearest texel (filter 0)
     float s = u - afloor(u);
@@ -536,10 +543,89 @@ static int texelOf(const Tex& t, float u, float v) {     // nearest texel (filte
     y = std::max(0, std::min(y, t.h - 1));
     return y * t.w + x;
 }
-static Color texRead(const Scene& sc, int tex, float u, float v) {
+static int texelAt(const Tex& t, float s, float tt) {    // Texture2D::read / ::pdf, filter 0
+    int x = (int)floorf(s * t.w);
+    int y = (int)floorf(tt * t.h);
+    if (y == t.h) y -= 1;
+    if (x == t.w) x -= 1;
+    x = std::max(0, std::min(x, t.w - 1));
+    y = std::max(0, std::min(y, t.h - 1));
+    return y * t.w + x;
+}
+
+// TriplanarTextureShader<Color>::evaluate (triplanarTextureShader.h:29-51) and <float>
+// (:71-93), as texel taps: axis i reads texel idx[i] with weight w[i] (w[i] = 0: skipped).
+struct TriTaps { int idx[3]; float w[3]; };
+static TriTaps triplanarTaps(const Scene& sc, const Tex& t, const LocalGeometry& lg, bool floatShader) {
+    const float* m = &sc.attrC2O[16 * (size_t)lg.attr];
+    float weights[3];
+    float weightsum = 0.f;
+    if (floatShader) {
+        const float ng[3] = {lg.Ng.x, lg.Ng.y, lg.Ng.z};
+        for (int i = 0; i < 3; ++i) {
+            weights[i] = fabsf(ng[i]);
+            weights[i] -= 0.2;
+            weights[i] = std::max(weights[i], 0.f);
+            weightsum += weights[i];
+        }
+    } else {
+        Vector N = normalize(Vector(m[0] * lg.Ng.x + m[1] * lg.Ng.y + m[2] * lg.Ng.z,
+                                    m[4] * lg.Ng.x + m[5] * lg.Ng.y + m[6] * lg.Ng.z,
+                                    m[8] * lg.Ng.x + m[9] * lg.Ng.y + m[10] * lg.Ng.z));
+        const float n[3] = {N.x, N.y, N.z};
+        for (int i = 0; i < 3; ++i) {
+            weights[i] = fabsf(n[i]);
+            weights[i] -= 0.25;
+            weights[i] = std::max(weights[i], 0.f);
+            weightsum += weights[i];
+        }
+    }
+    for (int i = 0; i < 3; ++i) weights[i] /= weightsum;
+    float xp = m[0] * lg.P.x + m[1] * lg.P.y + m[2] * lg.P.z + m[3];
+    float yp = m[4] * lg.P.x + m[5] * lg.P.y + m[6] * lg.P.z + m[7];
+    float zp = m[8] * lg.P.x + m[9] * lg.P.y + m[10] * lg.P.z + m[11];
+    float wp = m[12] * lg.P.x + m[13] * lg.P.y + m[14] * lg.P.z + m[15];
+    if (wp != 1.f) { float iw = 1.f / wp; xp *= iw; yp *= iw; zp *= iw; }
+    float inv = 1.f / t.triScale;                      // P /= m_scale
+    const float P[3] = {xp * inv, yp * inv, zp * inv};
+    TriTaps r;
+    for (int i = 0; i < 3; ++i) {
+        r.idx[i] = 0;
+        r.w[i] = 0.f;
+        if (weights[i] > 0) {
+            float s = fabsf(fmodf(P[(i + 1) % 3], 1.f));
+            float tt = fabsf(fmodf(P[(i + 2) % 3], 1.f));
+            r.idx[i] = texelAt(t, s, tt);
+            r.w[i] = weights[i];
+        }
+    }
+    return r;
+}
+// Shader<Color>::evaluate of a texture shader
+static Color shaderColor(const Scene& sc, int tex, const LocalGeometry& lg) {
     const Tex& t = sc.texs[tex];
-    const float* p = t.px + 3 * texelOf(t, u, v);
-    return Color(p[0], p[1], p[2]);
+    if (t.triScale == 0.f) {
+        const float* p = t.px + 3 * texelOf(t, lg.su, lg.sv);
+        return Color(p[0], p[1], p[2]);
+    }
+    const TriTaps k = triplanarTaps(sc, t, lg, false);
+    Color result(0.f);
+    for (int i = 0; i < 3; ++i)
+        if (k.w[i] > 0) {
+            const float* p = t.px + 3 * k.idx[i];
+            result += Color(p[0], p[1], p[2]) * k.w[i];
+        }
+    return result;
+}
+// Shader<float>::evaluate: the red channel
+static float shaderFloat(const Scene& sc, int tex, const LocalGeometry& lg) {
+    const Tex& t = sc.texs[tex];
+    if (t.triScale == 0.f) return t.px[3 * texelOf(t, lg.su, lg.sv)];
+    const TriTaps k = triplanarTaps(sc, t, lg, true);
+    float result = 0.f;
+    for (int i = 0; i < 3; ++i)
+        if (k.w[i] > 0) result += t.px[3 * k.idx[i]] * k.w[i];
+    return result;
 }
 
 // ------------------------------------------------------------ KelemenMaterial::getAlbedo (kelemenMaterial.cpp:180-212)
@@ -564,23 +650,24 @@ static float getAlbedo(const float* table, float costheta, float roughness) {
 
 // Material::getBrdf (matteMaterial.cpp:30-35, kelemenMaterial.cpp:214-255, metalMaterial.cpp:32-62,
 // constantMaterial.cpp:19-24)
-static BrdfState getBrdf(const Scene& sc, int matId, const Vector& Vn, const Vector& Nn, float su, float sv,
-                         bool mattePath, float lobeU) {
+static BrdfState getBrdf(const Scene& sc, int matId, const LocalGeometry& lg, bool mattePath, float lobeU) {
+    const Vector& Vn = lg.Vn;
+    const Vector& Nn = lg.Nn;
     const Mat& m = sc.mats[matId];
     BrdfState b;
     if (m.type == AUR_MAT_MATTE) {
-        b.type = MatteBrdf; b.color = m.diffTex >= 0 ? texRead(sc, m.diffTex, su, sv) : m.diff; b.roughness = 0;
+        b.type = MatteBrdf; b.color = m.diffTex >= 0 ? shaderColor(sc, m.diffTex, lg) : m.diff; b.roughness = 0;
         return b;
     }
     if (m.type == AUR_MAT_KELEMEN || m.type == AUR_MAT_COOKTORRANCE) {
-        float rough = m.roughTex >= 0 ? texRead(sc, m.roughTex, su, sv).r : m.rough;
+        float rough = m.roughTex >= 0 ? shaderFloat(sc, m.roughTex, lg) : m.rough;
         if (mattePath) rough = rough * (1. - CAUSTIC_BLUR) + CAUSTIC_BLUR;
-        b.type = SpecBrdf; b.color = m.specTex >= 0 ? texRead(sc, m.specTex, su, sv) : m.spec; b.roughness = rough;
+        b.type = SpecBrdf; b.color = m.specTex >= 0 ? shaderColor(sc, m.specTex, lg) : m.spec; b.roughness = rough;
         if (m.type == AUR_MAT_KELEMEN && m.refl < 1.f) {
             float albedo = getAlbedo(sc.albedo + (size_t)m.table * COS_ENTRIES * ROUGH_ENTRIES,
                                      clampf(dot(Nn, Vn), 0., 1.), rough);
             if (lobeU > albedo) {
-                b.type = MatteBrdf; b.color = m.diffTex >= 0 ? texRead(sc, m.diffTex, su, sv) : m.diff; b.roughness = 0;
+                b.type = MatteBrdf; b.color = m.diffTex >= 0 ? shaderColor(sc, m.diffTex, lg) : m.diff; b.roughness = 0;
             }
         }
         return b;
@@ -666,18 +753,9 @@ static Vector xformVector(const float* m, const Vector& v) {      // transform.c
     return Vector(m[0] * v.x + m[1] * v.y + m[2] * v.z, m[4] * v.x + m[5] * v.y + m[6] * v.z,
                   m[8] * v.x + m[9] * v.y + m[10] * v.z);
 }
-static int envTexel(const Tex& t, float s, float tt) {           // Texture2D::read / ::pdf, filter 0
-    int x = (int)floorf(s * t.w);
-    int y = (int)floorf(tt * t.h);
-    if (y == t.h) y -= 1;
-    if (x == t.w) x -= 1;
-    x = std::max(0, std::min(x, t.w - 1));
-    y = std::max(0, std::min(y, t.h - 1));
-    return y * t.w + x;
-}
 static Color envRead(const Scene& sc, const Light& l, float s, float tt) {
     const Tex& t = sc.texs[l.tex];
-    const float* p = t.px + 3 * envTexel(t, s, tt);
+    const float* p = t.px + 3 * texelAt(t, s, tt);
     return Color(p[0], p[1], p[2]);
 }
 static float envMapPdf(const Scene& sc, const Light& l, float s, float tt) {   // p.a / m_pdf_normalization
@@ -813,7 +891,6 @@ inline float PowerHeuristic(int nf, float fPdf, int ng, float gPdf) {   // integ
 }
 
 // ------------------------------------------------------------ Integrator (integrator.cpp)
-struct LocalGeometry { Point P; Vector Vn, Nn; float su, sv; int attr; };
 struct Counts { uint64_t closest = 0, shadow = 0; };
 
 static LocalGeometry hitGeometry(const Scene& sc, const Ray& ray, int prim, float t, float u, float v) {
@@ -832,8 +909,16 @@ static LocalGeometry hitGeometry(const Scene& sc, const Ray& ray, int prim, floa
         lg.sv = w * uv[1] + u * uv[3] + v * uv[5];
     }
     lg.attr = sc.triAttr[prim];
-    lg.Vn = -normalize(ray.direction);
+    lg.Ng = hitN;
     lg.Nn = hitN;
+    const Mat& m = sc.mats[sc.attrMat[lg.attr]];
+    if (m.normTex != -1) {                           // Material::runNormalShader (material.cpp:27-40)
+        Color map = m.normTex == -2 ? m.normC : shaderColor(sc, m.normTex, lg);
+        Vector Ns = tangentToWorld(Vector(map.r, map.g, map.b), lg.Ng);
+        if (Ns.x || Ns.y || Ns.z) lg.Nn = normalize(Ns);
+        else lg.Nn = lg.Ng;
+    }
+    lg.Vn = -normalize(ray.direction);
     if (dot(lg.Vn, lg.Nn) <= 0.) {
         Vector tmp = cross(lg.Nn, lg.Vn);
         lg.Nn = normalize(cross(lg.Vn, tmp));
@@ -965,7 +1050,7 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
         const int vtx = trueBounces;
         if (rayType == DiffuseRay) mattePath = true;
         if (rayType == CameraRay || rayType == MirrorRay) Lo += pathThroughput * sc.attrEmission[lg.attr];
-        BrdfState brdf = getBrdf(sc, sc.attrMat[lg.attr], lg.Vn, lg.Nn, lg.su, lg.sv, mattePath, rng(vdim(vtx, DIM_LOBE)));
+        BrdfState brdf = getBrdf(sc, sc.attrMat[lg.attr], lg, mattePath, rng(vdim(vtx, DIM_LOBE)));
         Lo += integrateDirect(sc, lg, brdf, rng, vtx, cnt) * pathThroughput;
         Sample3D cur = brdfGetSample(brdf, lg.Vn, lg.Nn, rng(vdim(vtx, DIM_BRDF)), rng(vdim(vtx, DIM_BRDF + 1)));
         if (cur.pdf <= 0.f) break;
@@ -1014,7 +1099,10 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
 // on. (The product evaluates the same quantity in reverse, by path replay.)
 // Parameter vector: per material m (diffuse r, g, b, roughness) at 4m..4m+3, then the
 // texel floats at 4 nmat + i.
-struct ParamRef { long base = -1; bool perChannel = false; double chain = 1.0; };
+// A vertex's parameter: n blocks base[k] weighted w[k] (a triplanar texture blends up to
+// three texels; everything else is one block of weight 1).
+struct ParamRef { int n = 0; long base[3] = {-1, -1, -1}; double w[3] = {1, 1, 1}; bool perChannel = false;
+                  double chain = 1.0; };
 
 static ParamRef paramOf(const Scene& sc, int matId, const BrdfState& b, const LocalGeometry& lg, bool mattePath,
                         float lobeU) {
@@ -1025,15 +1113,25 @@ static ParamRef paramOf(const Scene& sc, int matId, const BrdfState& b, const Lo
         p.perChannel = true;
         if (m.diffTex >= 0) {
             const Tex& t = sc.texs[m.diffTex];
-            p.base = 4 * (long)sc.mats.size() + (long)t.offset + 3 * texelOf(t, lg.su, lg.sv);
+            const long tbase = 4 * (long)sc.mats.size() + (long)t.offset;
+            if (t.triScale == 0.f) {
+                p.n = 1;
+                p.base[0] = tbase + 3 * texelOf(t, lg.su, lg.sv);
+            } else {                                 // d colour / d texel = the texel's weight
+                const TriTaps k = triplanarTaps(sc, t, lg, false);
+                for (int i = 0; i < 3; ++i)
+                    if (k.w[i] > 0) { p.base[p.n] = tbase + 3 * (long)k.idx[i]; p.w[p.n] = k.w[i]; ++p.n; }
+            }
         } else {
-            p.base = 4 * matId;
+            p.n = 1;
+            p.base[0] = 4 * matId;
         }
         return p;
     }
     if (b.type == SpecBrdf && m.roughTex < 0 &&
         (m.type == AUR_MAT_KELEMEN || m.type == AUR_MAT_COOKTORRANCE || (m.type == AUR_MAT_METAL && lobeU > m.mix))) {
-        p.base = 4 * matId + 3;                      // roughness; blurred on matte paths (kelemenMaterial.cpp:232-234)
+        p.n = 1;
+        p.base[0] = 4 * matId + 3;                   // roughness; blurred on matte paths (kelemenMaterial.cpp:232-234)
         p.chain = mattePath ? 1.0 - CAUSTIC_BLUR : 1.0;
     }
     return p;
@@ -1126,7 +1224,7 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         }
         const float lobeU = rng(vdim(vtx, DIM_LOBE));
         const int matId = sc.attrMat[lg.attr];
-        BrdfState brdf = getBrdf(sc, matId, lg.Vn, lg.Nn, lg.su, lg.sv, mattePath, lobeU);
+        BrdfState brdf = getBrdf(sc, matId, lg, mattePath, lobeU);
         const double T[3] = {pathThroughput.r, pathThroughput.g, pathThroughput.b};
         const double score = kelemenScore(sc, sc.mats[matId], lg, brdf, mattePath);
         if (score != 0.0) {
@@ -1142,10 +1240,11 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
             if (e.perChannel) for (int c = 0; c < 3; ++c) contrib.push_back({e.base + c, delta[c] * e.d[c] * Dd[c]});
             else contrib.push_back({e.base, delta[0] * e.d[0] * Dd[0] + delta[1] * e.d[1] * Dd[1] + delta[2] * e.d[2] * Dd[2]});
         }
-        if (pr.base >= 0) {
-            if (pr.perChannel) for (int c = 0; c < 3; ++c) contrib.push_back({pr.base + c, delta[c] * T[c] * dg.dAlbedo[c]});
-            else contrib.push_back({pr.base, pr.chain * (delta[0] * T[0] * dg.dRough[0] + delta[1] * T[1] * dg.dRough[1] +
-                                                          delta[2] * T[2] * dg.dRough[2])});
+        for (int k = 0; k < pr.n; ++k) {
+            if (pr.perChannel)
+                for (int c = 0; c < 3; ++c) contrib.push_back({pr.base[k] + c, pr.w[k] * delta[c] * T[c] * dg.dAlbedo[c]});
+            else contrib.push_back({pr.base[k], pr.chain * (delta[0] * T[0] * dg.dRough[0] + delta[1] * T[1] * dg.dRough[1] +
+                                                             delta[2] * T[2] * dg.dRough[2])});
         }
         Sample3D cur = brdfGetSample(brdf, lg.Vn, lg.Nn, rng(vdim(vtx, DIM_BRDF)), rng(vdim(vtx, DIM_BRDF + 1)));
         if (cur.pdf <= 0.f) break;
@@ -1173,7 +1272,7 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         const double w[3] = {(double)cur.color.r * cosl / cur.pdf, (double)cur.color.g * cosl / cur.pdf,
                              (double)cur.color.b * cosl / cur.pdf};
         double dw[3] = {0, 0, 0};
-        if (pr.base >= 0) {
+        if (pr.n > 0) {
             if (pr.perChannel) {
                 for (int c = 0; c < 3; ++c) dw[c] = (double)cosl / cur.pdf / M_PI;   // w_c = albedo_c / pi cos / pdf
             } else {
@@ -1182,9 +1281,9 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
             }
         }
         for (auto& e : dT) for (int c = 0; c < 3; ++c) e.d[c] *= w[c];
-        if (pr.base >= 0) {
-            const double add[3] = {T[0] * dw[0], T[1] * dw[1], T[2] * dw[2]};
-            addDT(dT, pr.base, pr.perChannel, add);
+        for (int k = 0; k < pr.n; ++k) {
+            const double add[3] = {pr.w[k] * T[0] * dw[0], pr.w[k] * T[1] * dw[1], pr.w[k] * T[2] * dw[2]};
+            addDT(dT, pr.base[k], pr.perChannel, add);
         }
         pathThroughput *= cur.color * dot(lg.Nn, cur.ray.direction) / cur.pdf;
         if (bounces > minDepth) continueProbability *= cur.color.lum() * dot(lg.Nn, cur.ray.direction) / cur.pdf;
@@ -1238,6 +1337,8 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
         mt.rough = md.roughness; mt.roughB = md.roughness_b; mt.refl = md.reflectance; mt.mix = md.mix;
         mt.diffTex = md.diffuse_tex; mt.specTex = md.specular_tex; mt.roughTex = md.roughness_tex;
         mt.ior = md.ior;
+        mt.normTex = md.normal_kind == AUR_NORMAL_TEXTURE ? md.normal_tex : md.normal_kind == AUR_NORMAL_CONSTANT ? -2 : -1;
+        mt.normC = Color(md.normal[0], md.normal[1], md.normal[2]);
         // KelemenMaterial ctor: modrefl = roundf(reflectance*20)/20 selects the cache (kelemenMaterial.cpp:49-52)
         mt.table = md.type == AUR_MAT_KELEMEN ? std::max(0, std::min(REFL_ENTRIES - 1, (int)roundf(md.reflectance * (REFL_ENTRIES - 1)))) : 0;
         sc->mats.push_back(mt);
@@ -1275,6 +1376,7 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
     size_t off = 0;
     for (uint32_t t = 0; t < d->ntex; ++t) {
         Tex tx; tx.w = d->tex_dims[2 * t]; tx.h = d->tex_dims[2 * t + 1]; tx.px = nullptr; tx.offset = off;
+        tx.triScale = d->tex_triplanar_scale ? d->tex_triplanar_scale[t] : 0.f;
         sc->texs.push_back(tx);
         off += 3 * (size_t)tx.w * tx.h;
     }
@@ -1291,6 +1393,13 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
                 lum += (p[0] + p[1] + p[2]) / 3.f;
             }
         l.pdfNorm = lum / (t.w * t.h);
+    }
+    sc->attrC2O.assign(16 * (size_t)d->nattr, 0.f);
+    if (d->attr_camera_to_object) {
+        sc->attrC2O.assign(d->attr_camera_to_object, d->attr_camera_to_object + 16 * (size_t)d->nattr);
+    } else {
+        for (uint32_t i = 0; i < d->nattr; ++i)
+            for (int k = 0; k < 4; ++k) sc->attrC2O[16 * (size_t)i + 5 * k] = 1.f;
     }
     sc->albedo = albedo;
     sc->fov = d->fov; sc->width = d->width; sc->height = d->height;
@@ -1518,10 +1627,11 @@ int oracle_kelemen_table(float reflectance, int samples, uint32_t seed, float* o
 // kind 7 light_pdf     in: light, o3, d3, mint, maxt                 (9) out: pdf, maxt (2)
 // kind 8 light_visible in: light, P3, N3                             (7) out: visible (1)
 // kind 9 get_brdf      in: material, V3, N3, su, sv, matte, lobe_u  (11) out: lobe, color3, rough (5)
+// kind 10 shade_point  in: triangle, t, u, v, o3, d3, matte, lobe_u (12) out: N3, Ng3, lobe, color3, rough (11)
 int oracle_shading_probe(void* h, int kind, const float* in, uint32_t n, float* out, const float* tables) {
-    static const int kIn[10] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11};
-    static const int kOut[10] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5};
-    if (kind < 0 || kind > 9) return -1;
+    static const int kIn[11] = {13, 14, 14, 3, 7, 2, 9, 9, 7, 11, 12};
+    static const int kOut[11] = {7, 3, 1, 1, 3, 1, 8, 2, 1, 5, 11};
+    if (kind < 0 || kind > 10) return -1;
     const Scene* sc = (const Scene*)h;
     if (kind >= 6 && !sc) return -2;
     for (uint32_t i = 0; i < n; ++i) {
@@ -1556,10 +1666,18 @@ int oracle_shading_probe(void* h, int kind, const float* in, uint32_t n, float* 
             o[0] = lightPdf(*sc, sc->lights[(int)q[0]], &r); o[1] = r.maxt;
         } else if (kind == 8) {
             o[0] = lightVisible(sc->lights[(int)q[0]], Point(q[1], q[2], q[3]), Vector(q[4], q[5], q[6])) ? 1.f : 0.f;
-        } else {
-            BrdfState b = getBrdf(*sc, (int)q[0], Vector(q[1], q[2], q[3]), Vector(q[4], q[5], q[6]), q[7], q[8],
-                                  q[9] != 0.f, q[10]);
+        } else if (kind == 9) {
+            LocalGeometry lg;
+            lg.P = Point(0, 0, 0); lg.Vn = Vector(q[1], q[2], q[3]); lg.Nn = lg.Ng = Vector(q[4], q[5], q[6]);
+            lg.su = q[7]; lg.sv = q[8]; lg.attr = 0;
+            BrdfState b = getBrdf(*sc, (int)q[0], lg, q[9] != 0.f, q[10]);
             o[0] = (float)b.type; o[1] = b.color.r; o[2] = b.color.g; o[3] = b.color.b; o[4] = b.roughness;
+        } else {
+            Ray r; r.origin = Point(q[4], q[5], q[6]); r.direction = Vector(q[7], q[8], q[9]);
+            LocalGeometry lg = hitGeometry(*sc, r, (int)q[0], q[1], q[2], q[3]);
+            BrdfState b = getBrdf(*sc, sc->attrMat[lg.attr], lg, q[10] != 0.f, q[11]);
+            o[0] = lg.Nn.x; o[1] = lg.Nn.y; o[2] = lg.Nn.z; o[3] = lg.Ng.x; o[4] = lg.Ng.y; o[5] = lg.Ng.z;
+            o[6] = (float)b.type; o[7] = b.color.r; o[8] = b.color.g; o[9] = b.color.b; o[10] = b.roughness;
         }
     }
     return 0;

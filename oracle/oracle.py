@@ -46,7 +46,7 @@ def lib() -> C.CDLL:
 
 
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<i4"), ("attr", "<i4")])
-PROBE_OUT = [7, 3, 1, 1, 3, 1, 8, 2, 1, 5]
+PROBE_OUT = [7, 3, 1, 1, 3, 1, 8, 2, 1, 5, 11]
 
 
 def rng_u01(seed, pixel, sample, dim) -> float:

@@ -92,3 +92,15 @@ def test_adjoint_matches_fp64_oracle_under_an_env_map(ctx, kelemen_tables, oracl
     gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (112, 150, 32, 32), 64, 2, 25, mode)
     _compare(gm, cm, "materials through glass")
     _compare(gt, ct, "texels through glass")
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_adjoint_matches_fp64_oracle_texture_shaders(ctx, kelemen_tables, oracle_lib, mode):
+    """Triplanar diffuse shaders (each texel's gradient weighted by its blend weight) under
+    normal maps: the ground, the sphere's diffuse lobe and the box."""
+    from aurora_b200 import scenes
+    data = scenes.shader_scene(128, 128, spp=64)
+    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (56, 72, 32, 32), 64, 3, 26, mode)
+    assert np.count_nonzero(ct) > 100
+    _compare(gm, cm, "materials (diffuse rgb, roughness)")
+    _compare(gt, ct, "texels")

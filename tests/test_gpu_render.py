@@ -95,6 +95,15 @@ def test_environment_map_with_kelemen(ctx, oracle_lib, kelemen_tables, mode):
     compare(g, mean, m2, 16)
 
 
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_texture_shaders_and_normal_maps(ctx, oracle_lib, kelemen_tables, mode):
+    """Triplanar colour and roughness shaders, a normal-map texture and a constant normal map."""
+    from aurora_b200 import scenes
+    data = scenes.shader_scene(96, 96)
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 8, mode=mode)
+    compare(g, mean, m2, 8)
+
+
 def test_terrain_small(ctx, oracle_lib, kelemen_tables):
     """The large-scene generator at reduced size (roulette, 16 materials, 4 lights, depth 8)."""
     from aurora_b200 import scenes

@@ -106,6 +106,20 @@ def test_lights_and_materials(ctx, oracle_lib, kelemen_tables):
     close(ctx.probe(9, mats, scene), osc.probe(9, mats), frac=1e-3)
 
 
+def test_shade_points_texture_shaders_and_normal_maps(ctx, oracle_lib, kelemen_tables):
+    """The hit's shading frame and Material::getBrdf (probe kind 10): interpolated normal,
+    normal-map texture and constant normal map, triplanar colour and float shaders."""
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    from shade_points import hit_records
+    data = scenes.shader_scene(32, 32)
+    scene = ab.Scene(ctx, data)
+    rec = hit_records(data, 20000, 43)
+    rec[:, 11] = np.random.default_rng(44).uniform(0, 1, rec.shape[0])   # both Kelemen lobes
+    close(ctx.probe(10, rec, scene), oracle_lib.OracleScene(data, kelemen_tables).probe(10, rec), frac=1e-3)
+    scene.close()
+
+
 def test_mirror_and_transmission_lobes(ctx, oracle_lib):
     """Glass lobes (SpecMirror, SpecTransmit): sampled directions, pdf 1, colour."""
     r = np.random.default_rng(31)

@@ -285,3 +285,23 @@ def test_env_light_seen_by_camera(oracle_lib):
     mean, _, _ = oracle_lib.OracleScene(data).render(4, 3, 3, 1)
     np.testing.assert_allclose(mean[..., :3], np.broadcast_to([300.0, 2.0, 1.0], (8, 8, 3)), rtol=1e-6)
     assert np.all(mean[..., 3] == 1.0)
+
+
+def test_texture_shaders_and_normal_maps_known_answers(oracle_lib):
+    """Triplanar colour and float shaders (object-space and camera-space weights), the uv
+    shader, a normal-map texture and a constant normal map at random hits of the
+    shader workload, against an independent float64 restatement (texel choices may flip
+    where float rounding crosses a texel edge: at most 1% of the records)."""
+    from aurora_b200 import scenes
+    from shade_points import expected, hit_records
+    data = scenes.shader_scene(32, 32, sphere_level=2)
+    rec = hit_records(data, 3000, 41)
+    got = oracle_lib.OracleScene(data, np.zeros((21, 64, 32), np.float32)).probe(10, rec)
+    want = expected(data, rec)
+    bad = np.any(np.abs(got - want) > 2e-5 + 2e-5 * np.abs(want), axis=1)
+    assert bad.mean() <= 0.01, (bad.sum(), got[bad][:2], want[bad][:2])
+    # every kind of shading point was exercised
+    attr = data.tri_attr[rec[:, 0].astype(np.int64)]
+    assert all(np.count_nonzero(attr == a) > 300 for a in range(5))
+    # the normal maps tilt the shading normal away from Ng
+    assert np.mean(np.sum(got[:, :3] * got[:, 3:6], 1) < 0.999) > 0.3

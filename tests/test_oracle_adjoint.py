@@ -93,3 +93,37 @@ def test_oracle_adjoint_through_glass_matches_fd(oracle_lib):
         fd = (_loss(oracle_lib, _perturbed_material(data, m, c, h), tables, w, spp, crop, seed) -
               _loss(oracle_lib, _perturbed_material(data, m, c, -h), tables, w, spp, crop, seed)) / (2 * h)
         assert abs(gm[m, c] - fd) <= 0.01 * abs(fd) + 1e-6, (m, c, gm[m, c], fd)
+
+
+def test_oracle_adjoint_triplanar_texel_matches_fd(oracle_lib):
+    """A texel of a triplanar diffuse shader (blended with its neighbours on the other
+    projection axes) under a normal map, against central differences."""
+    from aurora_b200 import scenes
+    data = scenes.shader_scene(64, 64, spp=4, sphere_level=3)
+    tables = np.zeros((21, 64, 32), np.float32)
+    w = np.random.default_rng(8).normal(size=(64, 64, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    crop, spp, seed = (20, 30, 32, 32), 4, 3
+    osc = oracle_lib.OracleScene(data, tables, use_bvh=True)
+    gm, gt = osc.adjoint(spp, 6, 6, seed, w, crop=crop)
+    sizes = [t.size for t in data.textures]
+    first = np.cumsum([0] + sizes)
+    for tex in (0, 2, 4):                                   # ground, sphere and box shaders (triplanar)
+        block = gt[first[tex]:first[tex + 1]]
+        assert np.count_nonzero(block) > 0
+        i = first[tex] + int(np.argmax(np.abs(block)))
+        h = 1e-2
+        fd = (_loss(oracle_lib, _perturbed_texel_any(data, i, h), tables, w, spp, crop, seed) -
+              _loss(oracle_lib, _perturbed_texel_any(data, i, -h), tables, w, spp, crop, seed)) / (2 * h)
+        assert abs(gt[i] - fd) <= 0.01 * abs(fd) + 1e-6, (tex, i, gt[i], fd)
+
+
+def _perturbed_texel_any(data, i, h):
+    d = copy.copy(data)
+    tex = [np.array(t, np.float32, copy=True) for t in data.textures]
+    sizes = np.cumsum([0] + [t.size for t in tex])
+    k = int(np.searchsorted(sizes, i, side="right") - 1)
+    flat = tex[k].reshape(-1)
+    flat[i - sizes[k]] = flat[i - sizes[k]] + h
+    d.textures = tex
+    return d

@@ -247,11 +247,54 @@ def test_texture_shader_and_kelemen_material(tmp_path):
     assert m.reflectance == np.float32(0.5) and m.roughness == np.float32(0.2)
 
 
+def test_triplanar_shader_normal_map_and_object_transform(tmp_path):
+    """triplanarTextureShader (scale), a normal map from a shader and a constant one, and
+    each attribute's cameraToObject (the inverse of its camera-space transform)."""
+    v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
+    write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
+    tex = np.random.default_rng(4).uniform(0, 1, size=(4, 8, 3)).astype(np.float32)
+    write_pfm(str(tmp_path / "t.pfm"), tex)
+    shaders = {"tri": {"attributetype": "color", "type": "triplanarTextureShader", "texturename": "t.pfm",
+                       "scale": 0.25},
+               "rough": {"attributetype": "float", "type": "triplanarTextureShader", "texturename": "t.pfm",
+                         "scale": 2.0},
+               "nrm": {"attributetype": "color", "type": "texture2DShader", "texturename": "t.pfm"}}
+    mats = {"m": {"type": "kelemenMaterial", "diffusecolor": "tri", "speccolor": [1, 1, 1], "reflectance": 0.5,
+                  "roughness": "rough", "normalmap": "nrm"},
+            "n": {"type": "matteMaterial", "color": [0.5, 0.5, 0.5], "normalmap": [0.1, 0.2, 0.9]}}
+    p = write_single(str(tmp_path), "q.obj", 0, materials=mats, shaders=shaders)
+    s = json.load(open(p))
+    s["objects"]["g"]["transforms"] = [{"translate": [0.5, -1, 2]}, {"rotateY": 30}, {"scale": [2, 2, 2]}]
+    s["objects"]["h"] = {"type": "geometry", "path": "q.obj", "name": "h", "material": "n", "transforms": [],
+                         "subdlevels": 0}
+    json.dump(s, open(p, "w"))
+    data, _, _ = scenes.load_scene_file(p)
+    names = sorted(shaders)                                        # shaders are visited in key order
+    np.testing.assert_array_equal(data.tex_triplanar_scale,
+                                  np.array([shaders[k].get("scale", 0.0) for k in names], np.float32))
+    m, n = data.materials[0], data.materials[1]
+    assert m.diffuse_tex == names.index("tri") and m.roughness_tex == names.index("rough")
+    assert m.normal_kind == _abi.NORMAL_TEXTURE and m.normal_tex == names.index("nrm")
+    assert n.normal_kind == _abi.NORMAL_CONSTANT and n.normal_tex == -1
+    np.testing.assert_array_equal(np.array(n.normal), np.array([0.1, 0.2, 0.9], np.float32))
+    # cameraToObject maps the camera-space corners back to the object's quad
+    assert data.attr_c2o.shape == (2, 16)
+    c2o = data.attr_c2o[0].reshape(4, 4).astype(np.float64)
+    P = corners(data)[data.tri_attr == 0].reshape(-1, 3).astype(np.float64)
+    obj = P @ c2o[:3, :3].T + c2o[:3, 3]
+    np.testing.assert_allclose(np.abs(obj[:, :2]), 1.0, atol=1e-5)
+    np.testing.assert_allclose(obj[:, 2], 0.0, atol=1e-5)
+
+
 @pytest.mark.parametrize("mutate,status", [
     (lambda s: s.pop("options"), _abi.ERR_PARSE),
     (lambda s: s["materials"].update({"m": {"type": "glassMaterial"}}), _abi.ERR_PARSE),
     (lambda s: s["materials"].update({"m": {"type": "matteMaterial", "color": [1, 1, 1], "normalmap": "n"}}),
-     _abi.ERR_UNSUPPORTED),
+     _abi.ERR_PARSE),
+    (lambda s: s.update({"shaders": {"t": {"attributetype": "color", "type": "triplanarTextureShader",
+                                           "texturename": "t.pfm", "scale": 0}}}), _abi.ERR_PARSE),
+    (lambda s: s.update({"shaders": {"t": {"attributetype": "color", "type": "noiseShader",
+                                           "texturename": "t.pfm"}}}), _abi.ERR_PARSE),
     (lambda s: s["objects"].update({"e": {"type": "envlight"}}), _abi.ERR_PARSE),
     (lambda s: s["objects"].update({"e": {"type": "envlight", "transforms": [], "exposure": 0, "color": [1, 1, 1],
                                           "envmap": "sky.exr"}}), _abi.ERR_UNSUPPORTED),
