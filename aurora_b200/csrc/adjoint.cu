@@ -22,6 +22,7 @@
 // Cook-Torrance lobes (Kelemen, Cook-Torrance, metal roughnessA); a diffuse
 // texture receives the diffuse gradient of the texel the lookup used. Gradients
 // are summed in FP32 with TwoSum-compensated atomics (shared, then global).
+#define AUR_MATH_OUT_OF_LINE 1
 #include "aur_capi_internal.h"
 
 namespace aur {
@@ -453,8 +454,8 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
 // Replay form (pass 2 only): one thread per item of a record pass (sample-major:
 // sl * npix + pixel, sample index p.sample_offset + s0 + sl). The wavefront engine's
 // record pass wrote the hit records rec[item][p.max_depth] and lo_raw[item].
-// 8 resident blocks of 128 threads (64 registers): 11% faster than 4 blocks (128
-// registers) despite a few spills
+// 8 resident blocks of 128 threads (64 registers). (A grid-stride loop over a resident
+// grid was 30% slower: the block scheduler already balances 128-thread blocks.)
 __global__ void __launch_bounds__(kAdjBlock, 8) k_adjoint_replay(DevScene sc, PathParams p, int s0, uint32_t items,
                                                               const float4* __restrict__ rec,
                                                               const float4* __restrict__ lo_raw,

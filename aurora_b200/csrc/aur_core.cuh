@@ -74,15 +74,24 @@ struct PathRng {
 // what the host's libm returns (to within its own <1 ulp), so device and CPU
 // restatement agree on BRDF values even where the Beckmann lobe amplifies a
 // 1-ulp difference (d ln D / d theta ~ 2 tan / m^2).
-AUR_HD float xexpf(float x) { return (float)exp((double)x); }
-AUR_HD float xlogf(float x) { return (float)log((double)x); }
-AUR_HD float xpowf(float x, float y) { return (float)pow((double)x, (double)y); }
-AUR_HD float xacosf(float x) { return (float)acos((double)x); }
-AUR_HD float xtanf(float x) { return (float)tan((double)x); }
-AUR_HD float xatanf(float x) { return (float)atan((double)x); }
-AUR_HD float xcosf(float x) { return (float)cos((double)x); }
-AUR_HD float xsinf(float x) { return (float)sin((double)x); }
-AUR_HD float xatan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
+// A translation unit that defines AUR_MATH_OUT_OF_LINE before including this header gets
+// them out of line: inlined at every call site, their double-precision bodies multiply the
+// code of the adjoint kernels, whose warps then stall on instruction fetch. (The forward
+// shading kernels are faster with them inlined.)
+#ifdef AUR_MATH_OUT_OF_LINE
+#define AUR_MATH static __host__ __device__ __noinline__
+#else
+#define AUR_MATH AUR_HD
+#endif
+AUR_MATH float xexpf(float x) { return (float)exp((double)x); }
+AUR_MATH float xlogf(float x) { return (float)log((double)x); }
+AUR_MATH float xpowf(float x, float y) { return (float)pow((double)x, (double)y); }
+AUR_MATH float xacosf(float x) { return (float)acos((double)x); }
+AUR_MATH float xtanf(float x) { return (float)tan((double)x); }
+AUR_MATH float xatanf(float x) { return (float)atan((double)x); }
+AUR_MATH float xcosf(float x) { return (float)cos((double)x); }
+AUR_MATH float xsinf(float x) { return (float)sin((double)x); }
+AUR_MATH float xatan2f(float y, float x) { return (float)atan2((double)y, (double)x); }
 
 // ---------------------------------------------------------------- float3 helpers
 AUR_HD float3 mk(float x, float y, float z) { float3 r; r.x = x; r.y = y; r.z = z; return r; }

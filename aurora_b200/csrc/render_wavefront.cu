@@ -1067,23 +1067,22 @@ aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film
     std::vector<BatchItem> items(1);
     items[0] = {sc, p, npix, nullptr, nullptr};
     if (wants_tuning(o)) {
-        if (!sc->wf_tuned) {
-            // A scene of the same shape (triangles, materials, lights, resolution, spp,
-            // depths) reuses the configuration tuned on this context before.
-            uint64_t sig = 1469598103934665603ull;
-            const uint64_t parts[8] = {sc->ntri, sc->h_mats.size(), sc->h_lights.size(), (uint64_t)sc->cam.w,
-                                       (uint64_t)sc->cam.h, (uint64_t)o->spp, (uint64_t)o->max_depth,
-                                       (uint64_t)(int64_t)o->min_depth};
-            for (uint64_t v : parts) sig = (sig ^ v) * 1099511628211ull;
-            auto it = sc->ctx->wf_scene_tuned.find(sig);
-            if (it == sc->ctx->wf_scene_tuned.end()) {
-                WfConfig t;
-                if ((st = autotune(sc->ctx, items, &t)) != AUR_OK) return st;
-                it = sc->ctx->wf_scene_tuned.emplace(sig, std::array<int, 3>{(int)t.pool, t.block, t.sort}).first;
-            }
-            sc->wf_pool = it->second[0]; sc->wf_block = it->second[1]; sc->wf_sort = it->second[2];
-            sc->wf_tuned = true;
+        // Tuned once per render shape (triangles, materials, lights, resolution, spp, depths)
+        // on this context: a scene rendered at another spp or depth is tuned for that too,
+        // and a new scene of the same shape reuses the configuration.
+        uint64_t sig = 1469598103934665603ull;
+        const uint64_t parts[8] = {sc->ntri, sc->h_mats.size(), sc->h_lights.size(), (uint64_t)sc->cam.w,
+                                   (uint64_t)sc->cam.h, (uint64_t)o->spp, (uint64_t)o->max_depth,
+                                   (uint64_t)(int64_t)o->min_depth};
+        for (uint64_t v : parts) sig = (sig ^ v) * 1099511628211ull;
+        auto it = sc->ctx->wf_scene_tuned.find(sig);
+        if (it == sc->ctx->wf_scene_tuned.end()) {
+            WfConfig t;
+            if ((st = autotune(sc->ctx, items, &t)) != AUR_OK) return st;
+            it = sc->ctx->wf_scene_tuned.emplace(sig, std::array<int, 3>{(int)t.pool, t.block, t.sort}).first;
         }
+        sc->wf_pool = it->second[0]; sc->wf_block = it->second[1]; sc->wf_sort = it->second[2];
+        sc->wf_tuned = true;
         cfg.pool = sc->wf_pool; cfg.block = sc->wf_block; cfg.sort = sc->wf_sort;
     }
     std::vector<float4*> films = {(float4*)fo.ptr};

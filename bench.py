@@ -41,6 +41,9 @@ def parse():
     p.add_argument("--profile", action="store_true",
                    help="render two 1-spp frames of the workload with a fixed wavefront configuration "
                         "(pool 2^20, block 128, sort on) and exit: the small case for ncu captures")
+    p.add_argument("--profile-adjoint", action="store_true",
+                   help="one wavefront path-replay adjoint of the differentiable workload at 64 spp (pool "
+                        "2^20, block 128, sort on) and exit: the small case for ncu captures of the adjoint")
     return p.parse_args()
 
 
@@ -114,9 +117,35 @@ def render_opts_for(data, mode, rank=0, count_work=0, spp=None):
                           count_work=count_work)
 
 
+def spread_rows(H, rows, offset=0):
+    """`rows` full-width rows spread evenly over the frame (so that sky, terrain and spheres
+    enter the sample in the frame's proportions), shifted by `offset` rows."""
+    stride = H / rows
+    return sorted({(int(j * stride) + offset) % H for j in range(rows)})
+
+
+def render_rows(osc, data, ys, cores):
+    """Renders rows `ys` of the workload on the CPU; returns the seconds taken."""
+    r = data.render
+    t0 = time.perf_counter()
+    for y in ys:
+        osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y, data.width, 1), threads=cores,
+                   want_m2=False)
+    return time.perf_counter() - t0
+
+
+def calibrate_rows(osc, data, cores, budget_s):
+    """Rows (spread over the frame) that take about `budget_s` on the CPU."""
+    H = data.height
+    probe = spread_rows(H, 8, H // 16)
+    per_row = max(render_rows(osc, data, probe, cores) / len(probe), 1e-4)
+    return int(max(1, min(H, budget_s / per_row)))
+
+
 def cpu_baseline(data, tables, budget_s=15.0):
-    """CPU restatement (oracle, all host threads) on a bounded sample: a band of full-width
-    rows at the workload's spp. Returns (paths/s, sample description, cores, build seconds)."""
+    """CPU restatement (oracle, all host threads) on a bounded sample: full-width rows spread
+    evenly over the frame at the workload's spp. Returns (paths/s, sample description, cores,
+    build seconds)."""
     from oracle import oracle
     cores = os.cpu_count() or 1
     t0 = time.perf_counter()
@@ -124,19 +153,12 @@ def cpu_baseline(data, tables, budget_s=15.0):
     build_s = time.perf_counter() - t0
     r = data.render
     W, H = data.width, data.height
-    # calibrate on one row, then size the band to the budget
-    y = H // 2
-    t0 = time.perf_counter()
-    osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y, W, 1), threads=cores, want_m2=False)
-    one = max(time.perf_counter() - t0, 1e-3)
-    rows = int(max(1, min(H // 2, budget_s / one)))
-    y0 = max(0, y - rows // 2)
-    t0 = time.perf_counter()
-    osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y0, W, rows), threads=cores,
-               want_m2=False)
-    dt = time.perf_counter() - t0
-    paths = W * rows * r["spp"]
-    return paths / dt, f"{W}x{rows} rows at y={y0} x {r['spp']} spp ({paths} paths, {dt:.1f} s)", cores, build_s
+    rows = calibrate_rows(osc, data, cores, budget_s)
+    ys = spread_rows(H, rows)
+    dt = render_rows(osc, data, ys, cores)
+    paths = W * len(ys) * r["spp"]
+    return (paths / dt, f"{W}x{len(ys)} rows spread over the frame x {r['spp']} spp ({paths} paths, {dt:.1f} s)",
+            cores, build_s)
 
 
 def adjoint_ratio(ab, _abi, torch, ctx, stream, steps=2, warmup=1):
@@ -200,25 +222,17 @@ def run_reference(args):
     osc = oracle.OracleScene(data, tables, use_bvh=True)
     r = data.render
     W, H = data.width, data.height
-    t0 = time.perf_counter()
-    osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, H // 2, W, 1), threads=cores,
-               want_m2=False)
-    one = max(time.perf_counter() - t0, 1e-3)
-    rows = int(max(1, min(H // 4, 20.0 / max(args.steps + args.warmup, 1) / one)))
-    for _ in range(args.warmup):
-        osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, 0, W, 1), threads=cores,
-                   want_m2=False)
-    times = []
+    rows = calibrate_rows(osc, data, cores, 20.0 / max(args.steps + args.warmup, 1))
+    for k in range(args.warmup):
+        render_rows(osc, data, spread_rows(H, max(1, rows // 4), 3 + k), cores)
+    times, paths = [], 0
     for k in range(args.steps):
-        y0 = (k * rows) % max(1, H - rows)
-        t0 = time.perf_counter()
-        osc.render(r["spp"], r["max_depth"], r["min_depth"], r["seed"], crop=(0, y0, W, rows), threads=cores,
-                   want_m2=False)
-        times.append(time.perf_counter() - t0)
-    paths = W * rows * r["spp"]
+        ys = spread_rows(H, rows, k)              # a different set of rows each step
+        times.append(render_rows(osc, data, ys, cores))
+        paths = W * len(ys) * r["spp"]
     ms = 1000 * statistics.mean(times)
     value = paths / (ms / 1000)
-    sample = f"{W}x{rows} full-width rows x {r['spp']} spp per step ({paths} paths)"
+    sample = f"{W}x{rows} full-width rows spread over the frame x {r['spp']} spp per step ({paths} paths)"
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "path samples/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generator)",
@@ -249,12 +263,33 @@ def run_profile_case(args):
     return 0
 
 
+def run_profile_adjoint(args):
+    """One wavefront adjoint of the differentiable workload (texture scene, 256x256) at 64 spp,
+    about 0.6 GB on the device, no timing output."""
+    import aurora_b200 as ab
+    from aurora_b200 import _abi, scenes
+    data = scenes.texture_scene()
+    ctx = ab.Context(0)
+    scene = ab.Scene(ctx, data)
+    dfilm = np.random.default_rng(8).normal(size=(data.height, data.width, 4)).astype(np.float32)
+    r = data.render
+    gm, gt, st = scene.adjoint(ab.render_opts(64, r["max_depth"], r["max_depth"], r["seed"],
+                                              mode=_abi.RENDER_WAVEFRONT, wf_pool=1 << 20, wf_block=128, wf_sort=1),
+                               dfilm)
+    print(json.dumps({"profile_case": "adjoint " + data.name, "tris": data.ntri, "stats": st}))
+    scene.close()
+    ctx.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
     if args.profile:
         return run_profile_case(args)
+    if args.profile_adjoint:
+        return run_profile_adjoint(args)
     import torch
     import aurora_b200 as ab
     from aurora_b200 import _abi
@@ -377,14 +412,18 @@ def main():
                                             data.corner_uvs, data.attr_material, data.attr_emission))
         host_film = np.zeros((H, W, 4), np.float32)
         e2e_steps = max(1, min(args.steps, 2))
+
+        def e2e_step():
+            sc2 = ab.Scene(ctx, data)
+            sc2.render(render_opts_for(data, modes[head], rank), out=host_film)
+            sc2.close()
+        e2e_step()                                  # warm-up (untimed)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(e2e_steps):
-            sc2 = ab.Scene(ctx, data)
-            sc2.render(render_opts_for(data, modes[head], rank), out=host_film)
-            sc2.close()
+            e2e_step()
         torch.cuda.synchronize()
         dt = (time.perf_counter() - t0) / e2e_steps
         if dist:
