@@ -83,7 +83,7 @@ class RenderStats(C.Structure):
                 ("paths", C.c_uint64), ("node_visits", C.c_uint64), ("tri_tests", C.c_uint64),
                 ("launches", C.c_uint64), ("kernel_ms", C.c_double), ("shadow_node_visits", C.c_uint64),
                 ("shadow_tri_tests", C.c_uint64), ("stage_ms", C.c_double * 5), ("wf_pool", C.c_int32),
-                ("wf_block", C.c_int32), ("wf_sort", C.c_int32), ("pad", C.c_int32)]
+                ("wf_block", C.c_int32), ("wf_sort", C.c_int32), ("node_bytes", C.c_int32)]
 
 
 vp = C.c_void_p

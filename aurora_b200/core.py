@@ -140,7 +140,7 @@ def _stats(s: _abi.RenderStats) -> dict:
             "kernel_ms": s.kernel_ms, "shadow_node_visits": s.shadow_node_visits,
             "shadow_tri_tests": s.shadow_tri_tests,
             "stage_ms": dict(zip(("regen", "extend", "sort", "shade", "shadow"), list(s.stage_ms))),
-            "wf_config": {"pool": s.wf_pool, "block": s.wf_block, "sort": s.wf_sort}}
+            "wf_config": {"pool": s.wf_pool, "block": s.wf_block, "sort": s.wf_sort}, "node_bytes": s.node_bytes}
 
 
 class Scene:

@@ -23,6 +23,14 @@ namespace aur {
 struct BvhNode { float4 a, b, c, d; };
 struct BvhTri { float4 p1, e1, e2; };
 
+// 4-wide node (128 bytes, one cache line) collapsed from the binary tree: the
+// four children's boxes as structure of arrays (lox = the four children's lo.x,
+// ...) and their refs in the binary tree's encoding (>= 0: 4-wide node index;
+// < 0: leaf ~(start << 5 | count)). The boxes are the binary tree's padded child
+// boxes, bit for bit. Unused slots have +inf boxes (never entered) and ref ~0 (an
+// empty leaf).
+struct BvhNode4 { float4 lox, hix, loy, hiy, loz, hiz; int4 ref; int4 pad; };
+
 struct DeviceBvh {
     BvhNode* nodes = nullptr;     // num_nodes records, root at 0
     BvhTri* tris = nullptr;       // num_tris records in leaf order
@@ -30,6 +38,9 @@ struct DeviceBvh {
     int num_tris = 0;
     int depth = 0;                // longest root-to-leaf path (interior levels + 1)
     float lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};   // scene bounds
+    BvhNode4* nodes4 = nullptr;   // the 4-wide form, root at 0 (same triangles)
+    int num_nodes4 = 0;
+    int depth4 = 0;               // 4-wide levels on the longest path
 };
 
 struct BvhBuildOptions {
@@ -45,5 +56,9 @@ struct BvhBuildOptions {
 cudaError_t bvh_build_device(const float* verts, const uint32_t* idx, int ntri, const BvhBuildOptions& opt,
                              DeviceBvh* out, cudaStream_t stream);
 void bvh_free_device(DeviceBvh* bvh, cudaStream_t stream);
+// Collapses the binary tree of `bvh` into its 4-wide form (nodes4): each 4-wide node
+// takes a binary node's two children and opens its largest-area interior child until
+// it holds four, level by level from the root.
+cudaError_t bvh_collapse4(DeviceBvh* bvh, cudaStream_t stream);
 
 }  // namespace aur

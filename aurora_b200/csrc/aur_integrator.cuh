@@ -19,6 +19,7 @@ namespace aur {
 struct DevScene {
     const BvhNode* nodes;
     const BvhTri* tris;
+    const BvhNode4* nodes4;   // the 4-wide form of the same tree, or null
     ShadeScene sh;
     Camera cam;
 };
@@ -48,7 +49,23 @@ __device__ __forceinline__ int pick_visible_light(const ShadeScene& sh, float3 P
     return -1;
 }
 
+// Traversal of the scene's binary (kWidth 2) or 4-wide (kWidth 4) tree.
+template <int kWidth>
+__device__ __forceinline__ bool trace_closest(const DevScene& sc, float3 o, float3 d, float mint, float maxt, Hit* h,
+                                              TraceWork& w) {
+    if constexpr (kWidth == 4) return bvh_trace4<false>(sc.nodes4, sc.tris, o, d, mint, maxt, h, w);
+    else return bvh_trace<false>(sc.nodes, sc.tris, o, d, mint, maxt, h, w);
+}
+template <int kWidth>
+__device__ __forceinline__ bool trace_occluded(const DevScene& sc, float3 o, float3 d, float mint, float maxt,
+                                               TraceWork& w) {
+    Hit h;
+    if constexpr (kWidth == 4) return bvh_trace4<true>(sc.nodes4, sc.tris, o, d, mint, maxt, &h, w);
+    else return bvh_trace<true>(sc.nodes, sc.tris, o, d, mint, maxt, &h, w);
+}
+
 // integrateDirect (integrator.cpp:100-130) with integrateDirectLight / integrateDirectMIS.
+template <int kWidth>
 __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Frame& f, const Brdf& brdf,
                                                    const PathRng& rng, int vtx, RayCounts& rc) {
     float3 res = mk(0.f, 0.f, 0.f);
@@ -63,7 +80,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
     if (brdf.lobe == LOBE_MATTE) {
         if (cost >= 0.f && ls.pdf > 0.f) {
             ++rc.shadow;
-            if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work))
+            if (!trace_occluded<kWidth>(sc, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work))
                 res += cdiv((ls.color * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
         }
     } else {
@@ -71,7 +88,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
             const float bp = brdf_pdf(brdf, ls.dir, f.V, f.N);
             if (bp > 0.f) {
                 ++rc.shadow;
-                if (!bvh_occluded(sc.nodes, sc.tris, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work)) {
+                if (!trace_occluded<kWidth>(sc, f.P, ls.dir, kRayBias, ls.maxt, rc.shadow_work)) {
                     const float w = power_heuristic(ls.pdf, bp);
                     res += cdiv(((ls.color * w) * brdf_eval(brdf, ls.dir, f.V, f.N)) * cost, ls.pdf);
                 }
@@ -85,7 +102,7 @@ __device__ __forceinline__ float3 integrate_direct(const DevScene& sc, const Fra
             const float lp = light_pdf(sc.sh, L, f.P, bs.dir, kRayBias, &maxt);
             if (lp > 0.f && bs.pdf > 0.f) {
                 ++rc.shadow;
-                if (!bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, maxt, rc.shadow_work)) {
+                if (!trace_occluded<kWidth>(sc, f.P, bs.dir, kRayBias, maxt, rc.shadow_work)) {
                     const float w = power_heuristic(bs.pdf, lp);
                     res += cdiv(((bs.color * w) * light_eval(sc.sh, L, bs.dir)) * cost, bs.pdf);
                 }
@@ -139,6 +156,7 @@ AUR_HD float3 firefly_clamp(float3 Lo) {
 }
 
 // One camera path; returns the clamped radiance, sets *alpha to 1 on a camera hit.
+template <int kWidth>
 __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathParams& p, int px, int py,
                                                  const PathRng& rng, RayCounts& rc, float* alpha) {
     RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
@@ -147,7 +165,7 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
     *alpha = 0.f;
     float3 Lo = mk(0.f, 0.f, 0.f);
     const float3 cam_d = ray.d;
-    if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+    if (!trace_closest<kWidth>(sc, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
         if (sc.sh.nenv == 0) return Lo;
         *alpha = 1.f;                       // environment seen directly: not firefly-filtered
         return env_radiance(sc.sh, cam_d);
@@ -165,7 +183,7 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         if (collects_emission(kind)) Lo += T * at.emission;
         const Brdf brdf = get_brdf(sc.sh, at.material, f, matte_path,
                                    rng.u(vertex_dim(vtx, kDimLobe)));
-        Lo += integrate_direct(sc, f, brdf, rng, vtx, rc) * T;
+        Lo += integrate_direct<kWidth>(sc, f, brdf, rng, vtx, rc) * T;
         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
         if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
@@ -175,7 +193,7 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         ray.mint = kRayBias;
         ray.maxt = bs.maxt;
         ++rc.closest;
-        if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+        if (!trace_closest<kWidth>(sc, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
             // a mirror ray that escapes sees the environment along the CAMERA ray's
             // direction, as integrator.cpp:262-274 evaluates it
             if (kind == RAY_MIRROR && sc.sh.nenv) Lo += env_radiance(sc.sh, cam_d) * T;

@@ -100,6 +100,86 @@ __device__ __forceinline__ bool bvh_trace(const BvhNode* __restrict__ nodes, con
     return best >= 0;
 }
 
+// The same traversal over the 4-wide tree (one 128-byte record per node visit; hit
+// children nearest first for closest hits, slot order for any hit).
+constexpr int kTraversalStack4Local = 96;
+template <bool kAnyHit>
+__device__ __forceinline__ bool bvh_trace4(const BvhNode4* __restrict__ nodes, const BvhTri* __restrict__ tris,
+                                           float3 o, float3 d, float mint, float maxt, Hit* hit, TraceWork& work) {
+    const float3 id = mk(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+    const float3 ood = mk(o.x * id.x, o.y * id.y, o.z * id.z);
+    const float box_tmin = mint > 0.f ? mint * 0.99999905f : mint * 1.00000095f;
+    const float kMiss = __int_as_float(0x7f800000);
+    float tbest = maxt;
+    float box_tmax = tbest * 1.00000095f;
+    int best = -1;
+    float bu = 0.f, bv = 0.f;
+    int stack[kTraversalStack4Local];
+    int sp = 0;
+    int node = 0;
+    while (true) {
+        if (node >= 0) {
+            ++work.nodes;
+            const BvhNode4* q = nodes + node;
+            const float4 lx = __ldg(&q->lox), hx = __ldg(&q->hix), ly = __ldg(&q->loy), hy = __ldg(&q->hiy);
+            const float4 lz = __ldg(&q->loz), hz = __ldg(&q->hiz);
+            const int4 rf = __ldg(&q->ref);
+            float t[4];
+            int r[4] = {rf.x, rf.y, rf.z, rf.w};
+            float tc;
+            t[0] = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            if (!kAnyHit) {
+                auto cx = [&](int i, int j) {
+                    if (t[j] < t[i]) { const float tt = t[i]; t[i] = t[j]; t[j] = tt; const int rr = r[i]; r[i] = r[j]; r[j] = rr; }
+                };
+                cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
+                if (t[0] != kMiss) {
+                    if (t[3] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[3];
+                    if (t[2] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[2];
+                    if (t[1] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[1];
+                    node = r[0];
+                    continue;
+                }
+            } else {
+                int next = -1;
+                bool any = false;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    if (t[c] == kMiss) continue;
+                    if (!any) { next = r[c]; any = true; }
+                    else if (sp < kTraversalStack4Local) stack[sp++] = r[c];
+                }
+                if (any) { node = next; continue; }
+            }
+        } else {
+            const int packed = ~node;
+            const int start = packed >> 5, end = start + (packed & 31);
+            for (int k = start; k < end; ++k) {
+                ++work.tris;
+                const float4 p = __ldg(&tris[k].p1);
+                const float4 e1 = __ldg(&tris[k].e1);
+                const float4 e2 = __ldg(&tris[k].e2);
+                float t, u, v;
+                if (tri_intersect(mk(p.x, p.y, p.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), o, d, mint, tbest,
+                                  &t, &u, &v)) {
+                    if (kAnyHit) return true;
+                    tbest = t; bu = u; bv = v;
+                    best = __float_as_int(p.w);
+                    box_tmax = tbest * 1.00000095f;
+                }
+            }
+        }
+        if (sp == 0) break;
+        node = stack[--sp];
+    }
+    if (kAnyHit) return false;
+    hit->t = tbest; hit->u = bu; hit->v = bv; hit->prim = best;
+    return best >= 0;
+}
+
 __device__ __forceinline__ bool bvh_closest(const BvhNode* nodes, const BvhTri* tris, float3 o, float3 d, float mint,
                                             float maxt, Hit* hit, TraceWork& work) {
     return bvh_trace<false>(nodes, tris, o, d, mint, maxt, hit, work);
@@ -107,6 +187,18 @@ __device__ __forceinline__ bool bvh_closest(const BvhNode* nodes, const BvhTri* 
 __device__ __forceinline__ bool bvh_occluded(const BvhNode* nodes, const BvhTri* tris, float3 o, float3 d, float mint,
                                              float maxt, TraceWork& work) {
     Hit h;
+    return bvh_trace<true>(nodes, tris, o, d, mint, maxt, &h, work);
+}
+// The 4-wide tree when there is one, else the binary tree.
+__device__ __forceinline__ bool bvh_closest(const BvhNode* nodes, const BvhNode4* nodes4, const BvhTri* tris, float3 o,
+                                            float3 d, float mint, float maxt, Hit* hit, TraceWork& work) {
+    if (nodes4) return bvh_trace4<false>(nodes4, tris, o, d, mint, maxt, hit, work);
+    return bvh_trace<false>(nodes, tris, o, d, mint, maxt, hit, work);
+}
+__device__ __forceinline__ bool bvh_occluded(const BvhNode* nodes, const BvhNode4* nodes4, const BvhTri* tris, float3 o,
+                                             float3 d, float mint, float maxt, TraceWork& work) {
+    Hit h;
+    if (nodes4) return bvh_trace4<true>(nodes4, tris, o, d, mint, maxt, &h, work);
     return bvh_trace<true>(nodes, tris, o, d, mint, maxt, &h, work);
 }
 
@@ -118,10 +210,14 @@ namespace aur {
 // memory laid out [depth][thread] (consecutive threads hit consecutive banks at
 // any mix of depths, one wavefront per warp access), deeper entries in local memory.
 constexpr int kSharedDepth = 24;   // all-local stacks measured 1.7% slower in k_extend
-struct LaneStack {
+// A 4-wide node pushes up to three entries: the stack of its traversal holds 96
+// (the collapse checks 3 x 4-wide depth + 1 against it).
+constexpr int kTraversalStack4 = 96;
+template <int kCap>
+struct LaneStackT {
     int* col;                       // &s_stack[threadIdx.x]
     int stride;                     // blockDim.x
-    int deep[kTraversalStack - kSharedDepth];
+    int deep[kCap - kSharedDepth];
     __device__ __forceinline__ void set(int i, int v) {
         if (i < kSharedDepth) col[i * stride] = v; else deep[i - kSharedDepth] = v;
     }
@@ -129,6 +225,8 @@ struct LaneStack {
         return i < kSharedDepth ? col[i * stride] : deep[i - kSharedDepth];
     }
 };
+using LaneStack = LaneStackT<kTraversalStack>;
+using LaneStack4 = LaneStackT<kTraversalStack4>;
 
 // Resumable traversal of one ray, for persistent kernels whose lanes take a new
 // ray as soon as theirs finishes (lane refill). Same visiting order, slack and
@@ -257,6 +355,109 @@ struct TraceState {
         if (sp == 0) return true;
         node = stack[--sp];
         return false;
+    }
+};
+
+
+// The same resumable while-while traversal over the 4-wide tree: a node visit loads
+// one 128-byte record, tests four boxes, and continues with the nearest hit child
+// while the other hit children go on the stack (closest hit: pushed farthest first;
+// any hit: in slot order). Boxes and the triangle test are the binary tree's, so the
+// closest hit equals it whenever the minimum is unique.
+template <bool kAnyHit>
+struct TraceState4 {
+    float3 o, d, id, ood;
+    float mint, tbest, box_tmin, box_tmax, bu, bv;
+    int node, sp, best;
+    bool hit_any;
+    int leaf;
+    static constexpr int kNone = INT_MIN;
+
+    __device__ __forceinline__ void begin(float3 o_, float3 d_, float mint_, float maxt_) {
+        o = o_; d = d_;
+        id = mk(safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z));
+        ood = mk(o.x * id.x, o.y * id.y, o.z * id.z);
+        mint = mint_;
+        box_tmin = mint > 0.f ? mint * 0.99999905f : mint * 1.00000095f;
+        tbest = maxt_;
+        box_tmax = tbest * 1.00000095f;
+        bu = bv = 0.f;
+        node = 0; sp = 0; best = -1;
+        leaf = kNone;
+        hit_any = false;
+    }
+
+    __device__ __forceinline__ void visit(const BvhNode4* __restrict__ nodes, LaneStack4& stack) {
+        const BvhNode4* q = nodes + node;
+        const float4 lx = __ldg(&q->lox), hx = __ldg(&q->hix), ly = __ldg(&q->loy), hy = __ldg(&q->hiy);
+        const float4 lz = __ldg(&q->loz), hz = __ldg(&q->hiz);
+        const int4 rf = __ldg(&q->ref);
+        const float kMiss = __int_as_float(0x7f800000);
+        float t[4];
+        int r[4] = {rf.x, rf.y, rf.z, rf.w};
+        float tc;
+        t[0] = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        if (!kAnyHit) {   // ascending by entry distance (misses last): a five-exchange network
+            auto cx = [&](int i, int j) {
+                if (t[j] < t[i]) { const float tt = t[i]; t[i] = t[j]; t[j] = tt; const int rr = r[i]; r[i] = r[j]; r[j] = rr; }
+            };
+            cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
+            if (t[0] == kMiss) { node = sp > 0 ? stack.get(--sp) : kNone; return; }
+            if (t[3] != kMiss && sp < kTraversalStack4) stack.set(sp++, r[3]);
+            if (t[2] != kMiss && sp < kTraversalStack4) stack.set(sp++, r[2]);
+            if (t[1] != kMiss && sp < kTraversalStack4) stack.set(sp++, r[1]);
+            node = r[0];
+        } else {
+            int next = kNone;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                if (t[c] == kMiss) continue;
+                if (next == kNone) next = r[c];
+                else if (sp < kTraversalStack4) stack.set(sp++, r[c]);
+            }
+            node = next != kNone ? next : (sp > 0 ? stack.get(--sp) : kNone);
+        }
+    }
+
+    // As TraceState::round: interior phase until every live lane holds a leaf, then the
+    // leaf phase. All 32 lanes of the warp must call it.
+    __device__ __forceinline__ bool round(const BvhNode4* __restrict__ nodes, const BvhTri* __restrict__ tris,
+                                          LaneStack4& stack, bool live) {
+        bool finished = !live;
+        if (live && leaf == kNone && node == kNone) finished = true;
+        while (true) {
+            bool searching = false;
+            if (!finished && node != kNone && node >= 0) visit(nodes, stack);
+            if (!finished && node != kNone && node < 0 && leaf == kNone) {   // postpone this leaf
+                leaf = node;
+                node = sp > 0 ? stack.get(--sp) : kNone;
+            }
+            if (!finished) searching = leaf == kNone && node != kNone;
+            if (!__any_sync(0xffffffffu, searching)) break;
+        }
+        if (!finished && leaf != kNone) {
+            const int packed = ~leaf;
+            const int start = packed >> 5, end = start + (packed & 31);
+            leaf = kNone;
+            for (int k = start; k < end; ++k) {
+                const float4 p = __ldg(&tris[k].p1);
+                const float4 e1 = __ldg(&tris[k].e1);
+                const float4 e2 = __ldg(&tris[k].e2);
+                float t, u, v;
+                if (tri_intersect(mk(p.x, p.y, p.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), o, d, mint, tbest,
+                                  &t, &u, &v)) {
+                    if (kAnyHit) { hit_any = true; return true; }
+                    tbest = t; bu = u; bv = v;
+                    best = __float_as_int(p.w);
+                    box_tmax = tbest * 1.00000095f;
+                }
+            }
+        }
+        if (finished) return live;
+        return leaf == kNone && node == kNone;
     }
 };
 

@@ -538,7 +538,120 @@ cudaError_t bvh_build_device(const float* verts, const uint32_t* idx, int n, con
 void bvh_free_device(DeviceBvh* bvh, cudaStream_t s) {
     if (bvh->nodes) cudaFreeAsync(bvh->nodes, s);
     if (bvh->tris) cudaFreeAsync(bvh->tris, s);
+    if (bvh->nodes4) cudaFreeAsync(bvh->nodes4, s);
     *bvh = DeviceBvh();
+}
+
+namespace {
+
+__device__ __forceinline__ void child_of(const BvhNode& nd, int k, float lo[3], float hi[3], int* ref) {
+    if (k == 0) {
+        lo[0] = nd.a.x; hi[0] = nd.a.y; lo[1] = nd.a.z; hi[1] = nd.a.w; lo[2] = nd.c.x; hi[2] = nd.c.y;
+        *ref = __float_as_int(nd.d.x);
+    } else {
+        lo[0] = nd.b.x; hi[0] = nd.b.y; lo[1] = nd.b.z; hi[1] = nd.b.w; lo[2] = nd.c.z; hi[2] = nd.c.w;
+        *ref = __float_as_int(nd.d.y);
+    }
+}
+
+__device__ __forceinline__ float half_area(const float lo[3], const float hi[3]) {
+    const float dx = hi[0] - lo[0], dy = hi[1] - lo[1], dz = hi[2] - lo[2];
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// One level of the collapse: front[i] = (binary node, its 4-wide index). Interior
+// children get the next 4-wide indices and form the next level's front.
+__global__ void k_collapse4(const BvhNode* __restrict__ n2, const int2* __restrict__ front, int nfront,
+                            BvhNode4* __restrict__ out, int* counters, int2* __restrict__ next, int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfront) return;
+    const int2 f = front[i];
+    float lo[4][3], hi[4][3];
+    int ref[4];
+    int n = 2;
+    {
+        const BvhNode nd = n2[f.x];
+        child_of(nd, 0, lo[0], hi[0], &ref[0]);
+        child_of(nd, 1, lo[1], hi[1], &ref[1]);
+    }
+    while (n < 4) {
+        int best = -1;
+        float ba = -1.f;
+        for (int k = 0; k < n; ++k) {
+            if (ref[k] < 0) continue;
+            const float a = half_area(lo[k], hi[k]);
+            if (a > ba) { ba = a; best = k; }
+        }
+        if (best < 0) break;
+        const BvhNode c = n2[ref[best]];
+        child_of(c, 1, lo[n], hi[n], &ref[n]);
+        child_of(c, 0, lo[best], hi[best], &ref[best]);
+        ++n;
+    }
+    float v[6][4];
+    int r[4];
+    for (int k = 0; k < 4; ++k) {
+        if (k >= n) {
+            for (int d = 0; d < 6; ++d) v[d][k] = __int_as_float(0x7f800000);   // +inf: never entered
+            r[k] = ~0;
+            continue;
+        }
+        v[0][k] = lo[k][0]; v[1][k] = hi[k][0]; v[2][k] = lo[k][1];
+        v[3][k] = hi[k][1]; v[4][k] = lo[k][2]; v[5][k] = hi[k][2];
+        if (ref[k] >= 0) {
+            const int j = atomicAdd(&counters[0], 1);
+            const int q = atomicAdd(&counters[1], 1);
+            if (j < cap && q < cap) next[q] = make_int2(ref[k], j);
+            r[k] = j;
+        } else {
+            r[k] = ref[k];
+        }
+    }
+    if (f.y >= cap) return;
+    BvhNode4 o;
+    o.lox = make_float4(v[0][0], v[0][1], v[0][2], v[0][3]);
+    o.hix = make_float4(v[1][0], v[1][1], v[1][2], v[1][3]);
+    o.loy = make_float4(v[2][0], v[2][1], v[2][2], v[2][3]);
+    o.hiy = make_float4(v[3][0], v[3][1], v[3][2], v[3][3]);
+    o.loz = make_float4(v[4][0], v[4][1], v[4][2], v[4][3]);
+    o.hiz = make_float4(v[5][0], v[5][1], v[5][2], v[5][3]);
+    o.ref = make_int4(r[0], r[1], r[2], r[3]);
+    o.pad = make_int4(0, 0, 0, 0);
+    out[f.y] = o;
+}
+
+}  // namespace
+
+cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
+    if (!b->nodes || b->num_nodes < 1) return cudaErrorInvalidValue;
+    const int cap = b->num_nodes;             // a 4-wide tree has at most as many nodes as the binary one
+    int2 *fa = nullptr, *fb = nullptr;
+    int* counters = nullptr;
+    CK(dalloc(&b->nodes4, cap, s));
+    CK(dalloc(&fa, cap, s));
+    CK(dalloc(&fb, cap, s));
+    CK(dalloc(&counters, 2, s));
+    const int2 root = make_int2(0, 0);
+    const int init[2] = {1, 0};
+    CK(cudaMemcpyAsync(fa, &root, sizeof(int2), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, s));
+    int nfront = 1, levels = 0, hc[2] = {1, 0};
+    while (nfront > 0) {
+        if (++levels > 64) return cudaErrorUnknown;   // the binary tree's depth is at most 63
+        CK(cudaMemsetAsync(counters + 1, 0, sizeof(int), s));
+        k_collapse4<<<div_up(nfront, 256), 256, 0, s>>>(b->nodes, fa, nfront, b->nodes4, counters, fb, cap);
+        CK(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        if (hc[0] > cap || hc[1] > cap) return cudaErrorUnknown;
+        nfront = hc[1];
+        std::swap(fa, fb);
+    }
+    b->num_nodes4 = hc[0];
+    b->depth4 = levels;
+    dfree(fa, s);
+    dfree(fb, s);
+    dfree(counters, s);
+    return cudaGetLastError();
 }
 
 }  // namespace aur

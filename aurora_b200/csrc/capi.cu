@@ -142,6 +142,17 @@ aur_status aur_ctx_create(int device, aur_ctx** out) {
     c->own_stream = true;
     e = cudaMalloc(&c->counters, sizeof(unsigned long long) * 8);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->work_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        // Scene and BVH buffers come from the device's stream-ordered pool; keeping freed
+        // blocks reserved (instead of trimming at every synchronisation) makes a new scene's
+        // allocations reuse them rather than map fresh memory. aur_ctx_destroy trims it.
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_order, cudaEventDisableTiming);
     if (e != cudaSuccess) {
         if (c->counters) cudaFree(c->counters);
@@ -168,6 +179,12 @@ aur_status aur_ctx_destroy(aur_ctx* ctx) {
     if (ctx->work_stream) { cudaStreamSynchronize(ctx->work_stream); cudaStreamDestroy(ctx->work_stream); }
     if (ctx->ev_order) cudaEventDestroy(ctx->ev_order);
     if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, ctx->device) == cudaSuccess) {
+        cudaDeviceSynchronize();
+        cudaMemPoolTrimTo(pool, 0);
+    }
+    cudaGetLastError();
     delete ctx;
     return AUR_OK;
 }
@@ -219,6 +236,13 @@ aur_status aur_bvh_build(aur_ctx* ctx, const float* verts, uint32_t nvert, const
         bvh_free_device(&b->bvh, s);
         delete b;
         return fail(AUR_ERR_UNSUPPORTED, "aur_bvh_build: tree deeper than the traversal stack");
+    }
+    if (e == cudaSuccess) e = bvh_collapse4(&b->bvh, s);
+    if (e == cudaSuccess && 3 * b->bvh.depth4 + 1 > kTraversalStack4) {
+        // a 4-wide node pushes up to three entries: too deep for its stack, keep the binary tree only
+        cudaFreeAsync(b->bvh.nodes4, s);
+        b->bvh.nodes4 = nullptr;
+        b->bvh.num_nodes4 = 0;
     }
     if (e == cudaSuccess && tri_attr) {
         e = cudaMallocAsync(&b->tri_attr, sizeof(int) * ntri, s);

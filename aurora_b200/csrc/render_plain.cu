@@ -26,7 +26,11 @@ __device__ __forceinline__ void add_counters(unsigned long long* counters, const
         for (int k = 0; k < kN; ++k) atomicAdd(&counters[k], v[k]);
 }
 
-template <bool kFp64, bool kCount>
+// kWidth: the tree traversed (2 binary, 4 four-wide). The timed kernels use the binary
+// tree, on which this one-thread-per-path kernel is fastest (its code holds five
+// traversals; the 4-wide ones made it 30% slower); the counting pass can use either, to
+// count the work of the wavefront renderer's traversal.
+template <bool kFp64, bool kCount, int kWidth>
 __global__ void __launch_bounds__(kPlainBlock) k_render_plain(DevScene sc, PathParams p, float4* film,
                                                               double* film64, unsigned long long* counters) {
     const int npix = sc.cam.w * sc.cam.h;
@@ -44,7 +48,7 @@ __global__ void __launch_bounds__(kPlainBlock) k_render_plain(DevScene sc, PathP
         for (int s = 0; s < p.spp; ++s) {
             rng.base = path_base((uint32_t)pixel, (uint32_t)(p.sample_offset + s));
             float a;
-            const float3 L = integrate_path(sc, p, px, py, rng, rc, &a);
+            const float3 L = integrate_path<kWidth>(sc, p, px, py, rng, rc, &a);
             if (kFp64) { d[0] += L.x; d[1] += L.y; d[2] += L.z; }
             else acc.add(L);
             alpha_sum += a;
@@ -79,9 +83,10 @@ cudaError_t launch_render_plain(const DevScene& sc, const PathParams& p, float4*
                                 unsigned long long* counters, bool count_work, cudaStream_t s) {
     const int npix = sc.cam.w * sc.cam.h;
     const int grid = (npix + kPlainBlock - 1) / kPlainBlock;
-    if (film64) k_render_plain<true, false><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
-    else if (count_work) k_render_plain<false, true><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
-    else k_render_plain<false, false><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    if (film64) k_render_plain<true, false, 2><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else if (count_work && sc.nodes4) k_render_plain<false, true, 4><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else if (count_work) k_render_plain<false, true, 2><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else k_render_plain<false, false, 2><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
     return cudaGetLastError();
 }
 

@@ -26,6 +26,7 @@
 #include <memory>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 
 namespace aur {
 namespace {
@@ -213,8 +214,11 @@ __device__ __forceinline__ int bucket_of(const ShadeScene& sh, int prim) {
 // Closest hit for the extension queue. Each lane keeps a resumable traversal;
 // finished lanes are refilled from the queue (one atomic per warp) while the
 // others continue, so a warp is not held up by its slowest ray.
-template <bool kSort>
+template <bool kSort, bool kWide>
 __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_q) {
+    using Stack = std::conditional_t<kWide, LaneStack4, LaneStack>;
+    using Trace = std::conditional_t<kWide, TraceState4<false>, TraceState<false>>;
+    using Node = std::conditional_t<kWide, BvhNode4, BvhNode>;
     const uint32_t* qin = in_q ? w.q_ext1 : w.q_ext0;
     const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
     // Outputs of the later stages start empty. Only counters that no block of
@@ -232,11 +236,11 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
     __shared__ uint32_t s_bucket[kBuckets];   // per-block material counts, added to the global ones at exit
     if (kSort && threadIdx.x < kBuckets) s_bucket[threadIdx.x] = 0;
     __syncthreads();
-    LaneStack stack;
+    Stack stack;
     stack.col = s_stack + threadIdx.x;
     stack.stride = blockDim.x;
-    TraceState<false> ts;
-    const BvhNode* nodes = nullptr;
+    Trace ts;
+    const Node* nodes = nullptr;
     const BvhTri* tris = nullptr;
     const WfScene* S = nullptr;
     uint32_t slot = 0;
@@ -255,7 +259,8 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
                 if (k < n) {
                     slot = qin[k];
                     S = &w.scenes[w.id[slot].x];
-                    nodes = S->sc.nodes;
+                    if constexpr (kWide) nodes = S->sc.nodes4;
+                    else nodes = S->sc.nodes;
                     tris = S->sc.tris;
                     const float4 o = w.ray_o[slot], d = w.ray_d[slot];
                     ts.begin(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, d.w);
@@ -502,15 +507,19 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
 // ------------------------------------------------------------------ shadow
 // Occlusion of the next-event rays (entries slot << 1 | ray); lanes are refilled as in
 // k_extend. An unoccluded ray sets its bit in sh_vis; the next regen adds the light.
+template <bool kWide>
 __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_shadow(WfPool w) {
+    using Stack = std::conditional_t<kWide, LaneStack4, LaneStack>;
+    using Trace = std::conditional_t<kWide, TraceState4<true>, TraceState<true>>;
+    using Node = std::conditional_t<kWide, BvhNode4, BvhNode>;
     const uint32_t n = w.ctr[C_SHADOW];
     if (blockIdx.x == 0 && threadIdx.x == 0) w.rays[1] += n;
     extern __shared__ int s_stack[];
-    LaneStack stack;
+    Stack stack;
     stack.col = s_stack + threadIdx.x;
     stack.stride = blockDim.x;
-    TraceState<true> ts;
-    const BvhNode* nodes = nullptr;
+    Trace ts;
+    const Node* nodes = nullptr;
     const BvhTri* tris = nullptr;
     uint32_t entry = 0;
     bool has = false, exhausted = false;
@@ -529,7 +538,8 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_shadow(WfPool w) {
                     entry = w.q_shadow[k];
                     const uint32_t slot = entry >> 1;
                     const WfScene& S = w.scenes[w.id[slot].x];
-                    nodes = S.sc.nodes;
+                    if constexpr (kWide) nodes = S.sc.nodes4;
+                    else nodes = S.sc.nodes;
                     tris = S.sc.tris;
                     const float4 p = w.sh_p[slot];
                     const float4 d = (entry & 1u) ? w.sh_d1[slot] : w.sh_d0[slot];
@@ -589,7 +599,15 @@ struct WfConfig {
     int block = 128;
     int sort = 1;
     int record = 0;   // record mode: hit records + unclamped radiance per item instead of samples
+    int wide = 0;     // traverse the 4-wide trees (every scene of the batch has one)
 };
+
+// The 4-wide traversal is used when every scene of a batch has a 4-wide tree.
+#ifndef AUR_WIDE_TRAVERSAL
+#define AUR_WIDE_TRAVERSAL 1
+#endif
+struct BatchItem;
+static int wide_for(const std::vector<BatchItem>& items);
 
 // ------------------------------------------------------------------ host driver
 struct WfRun {
@@ -655,9 +673,11 @@ struct WfRun {
             cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, c.block, smem);
             return std::max(1, nb) * sms;
         };
-        grid_ext = persist(c.sort ? (const void*)k_extend<true> : (const void*)k_extend<false>, stack_smem);
+        const void* ext = c.wide ? (c.sort ? (const void*)k_extend<true, true> : (const void*)k_extend<false, true>)
+                                 : (c.sort ? (const void*)k_extend<true, false> : (const void*)k_extend<false, false>);
+        grid_ext = persist(ext, stack_smem);
         grid_shade = persist(c.record ? (const void*)k_shade<true> : (const void*)k_shade<false>, 0);
-        grid_shadow = persist((const void*)k_shadow, stack_smem);
+        grid_shadow = persist(c.wide ? (const void*)k_shadow<true> : (const void*)k_shadow<false>, stack_smem);
         grid_sort = persist((const void*)k_sort_scatter, 0);
         grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 16);
         return cudaSuccess;
@@ -670,15 +690,21 @@ struct WfRun {
         if (cfg.record) k_regen<true><<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
         else k_regen<false><<<grid_regen, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[0], stream, cudaEventRecordExternal);
-        if (cfg.sort) k_extend<true><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
-        else k_extend<false><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
+        if (cfg.wide) {
+            if (cfg.sort) k_extend<true, true><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
+            else k_extend<false, true><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
+        } else {
+            if (cfg.sort) k_extend<true, false><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
+            else k_extend<false, false><<<grid_ext, cfg.block, stack_smem, stream>>>(w, in_q);
+        }
         cudaEventRecordWithFlags(e[1], stream, cudaEventRecordExternal);
         if (cfg.sort) k_sort_scatter<<<grid_sort, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[2], stream, cudaEventRecordExternal);
         if (cfg.record) k_shade<true><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
         else k_shade<false><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
         cudaEventRecordWithFlags(e[3], stream, cudaEventRecordExternal);
-        k_shadow<<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
+        if (cfg.wide) k_shadow<true><<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
+        else k_shadow<false><<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
         cudaEventRecordWithFlags(e[4], stream, cudaEventRecordExternal);
     }
 
@@ -834,6 +860,7 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
                 c.pool = pools[pi];
                 c.block = blocks[bi];
                 c.sort = so;
+                c.wide = wide_for(items);
                 WfRun run;
                 e = run.init(c, (int)items.size(), s);
                 if (e == cudaSuccess)
@@ -864,11 +891,11 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
 // Engines (pool buffers, captured graph, events, sample buffer) are cached per
 // (context, configuration) and reused by later calls; aur_ctx_destroy releases them.
 static std::mutex g_engine_mutex;
-static std::map<std::tuple<aur_ctx*, uint32_t, int, int, int>, std::unique_ptr<WfRun>> g_engines;
+static std::map<std::tuple<aur_ctx*, uint32_t, int, int, int, int>, std::unique_ptr<WfRun>> g_engines;
 
 static WfRun* engine_for(aur_ctx* ctx, const WfConfig& cfg, int nscenes, cudaError_t* err) {
     std::lock_guard<std::mutex> lock(g_engine_mutex);
-    const auto key = std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort, cfg.record);
+    const auto key = std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort, cfg.record, cfg.wide);
     auto it = g_engines.find(key);
     if (it != g_engines.end() && it->second->cap_scenes >= nscenes) return it->second.get();
     if (it != g_engines.end()) { it->second->release(); g_engines.erase(it); }
@@ -882,7 +909,7 @@ static WfRun* engine_for(aur_ctx* ctx, const WfConfig& cfg, int nscenes, cudaErr
 
 static void wf_drop_engine(aur_ctx* ctx, const WfConfig& cfg) {
     std::lock_guard<std::mutex> lock(g_engine_mutex);
-    auto it = g_engines.find(std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort, cfg.record));
+    auto it = g_engines.find(std::make_tuple(ctx, cfg.pool, cfg.block, cfg.sort, cfg.record, cfg.wide));
     if (it != g_engines.end()) { it->second->release(); g_engines.erase(it); }
 }
 
@@ -894,10 +921,19 @@ void wf_release_context(aur_ctx* ctx) {
     }
 }
 
+static int wide_for(const std::vector<BatchItem>& items) {
+    if (!AUR_WIDE_TRAVERSAL) return 0;
+    for (const BatchItem& it : items)
+        if (!it.scene->bvh.bvh.nodes4) return 0;
+    return 1;
+}
+
 // Renders a batch of scenes with the wavefront engine. films[i]: device float4[npix].
-static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, const WfConfig& cfg,
+static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, const WfConfig& cfg_in,
                                   std::vector<float4*>& films, aur_render_stats* stats, float* kernel_ms) {
     const int n = (int)items.size();
+    WfConfig cfg = cfg_in;
+    cfg.wide = wide_for(items);
     // The engine runs on the context's own non-blocking stream (graph capture is not
     // allowed on the legacy default stream), ordered after the caller's stream.
     cudaStream_t s = ctx->work_stream;
@@ -985,6 +1021,7 @@ static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, c
         stats->wf_pool = (int32_t)cfg.pool;
         stats->wf_block = cfg.block;
         stats->wf_sort = cfg.sort;
+        stats->node_bytes = cfg.wide ? (int32_t)sizeof(BvhNode4) : (int32_t)sizeof(BvhNode);
     }
     return AUR_OK;
 }
@@ -999,6 +1036,9 @@ aur_status wf_record_pass(aur_scene* sc, const PathParams& p, int s0, int nsampl
     WfConfig cfg;
     if (sc->wf_tuned) { cfg.pool = (uint32_t)sc->wf_pool; cfg.block = sc->wf_block; cfg.sort = sc->wf_sort; }
     cfg.record = 1;
+    std::vector<BatchItem> items(1);
+    items[0] = {sc, p, (uint32_t)sc->cam.w * (uint32_t)sc->cam.h, nullptr, nullptr};
+    cfg.wide = wide_for(items);
     cudaStream_t s = ctx->work_stream;
     cudaEventRecord(ctx->ev_order, ctx->stream);
     cudaStreamWaitEvent(s, ctx->ev_order, 0);
@@ -1006,8 +1046,6 @@ aur_status wf_record_pass(aur_scene* sc, const PathParams& p, int s0, int nsampl
     WfRun* engine = engine_for(ctx, cfg, 1, &e);
     if (!engine) return cuda_fail(e, "adjoint record pass: pool allocation");
     WfRun& run = *engine;
-    std::vector<BatchItem> items(1);
-    items[0] = {sc, p, (uint32_t)sc->cam.w * (uint32_t)sc->cam.h, nullptr, nullptr};
     std::vector<WfScene> tab;
     const uint32_t total = fill_table(items, s0, nsamples, nullptr, tab, run.cap_scenes);
     tab[0].rec = rec;

@@ -97,7 +97,7 @@ template <typename T>
 static cudaError_t upload(T** dst, const void* src, size_t count, cudaStream_t s) {
     *dst = nullptr;
     if (!src || count == 0) return cudaSuccess;
-    cudaError_t e = cudaMalloc((void**)dst, sizeof(T) * count);
+    cudaError_t e = cudaMallocAsync((void**)dst, sizeof(T) * count, s);
     if (e != cudaSuccess) return e;
     return cudaMemcpyAsync(*dst, src, sizeof(T) * count,
                            is_device_ptr(src) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s);
@@ -111,7 +111,8 @@ static void scene_free(aur_scene* sc) {
     cudaStreamSynchronize(s);
     void* bufs[] = {sc->bvh.tri_attr, sc->corner_n, sc->corner_uv, sc->attrs, sc->mats, sc->lights, sc->texs, sc->texels,
                     sc->attr_c2o};
-    for (void* b : bufs) if (b) cudaFree(b);
+    for (void* b : bufs) if (b) cudaFreeAsync(b, s);
+    cudaStreamSynchronize(s);
     delete sc;
 }
 
@@ -121,6 +122,7 @@ DevScene aur_scene::dev() const {
     DevScene d;
     d.nodes = bvh.bvh.nodes;
     d.tris = bvh.bvh.tris;
+    d.nodes4 = bvh.bvh.nodes4;
     d.sh.mats = mats;
     d.sh.attrs = attrs;
     d.sh.lights = lights;
@@ -403,6 +405,7 @@ static aur_status render_plain_impl(aur_scene* sc, const aur_render_opts* o, voi
         stats->shadow_tri_tests = cnt[7];
         stats->launches = 1;
         stats->kernel_ms = ms;
+        stats->node_bytes = o->count_work && sc->bvh.bvh.nodes4 ? (int32_t)sizeof(BvhNode4) : (int32_t)sizeof(BvhNode);
     }
     return AUR_OK;
 }

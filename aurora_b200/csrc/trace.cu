@@ -11,6 +11,7 @@ namespace {
 constexpr int kTraceBlock = 128;
 
 __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(const BvhNode* __restrict__ nodes,
+                                                               const BvhNode4* __restrict__ nodes4,
                                                                const BvhTri* __restrict__ tris,
                                                                const int* __restrict__ tri_attr,
                                                                const float4* __restrict__ rays, float* hits,
@@ -21,7 +22,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(const BvhNode* __
     const float4 b = __ldg(&rays[2 * i + 1]);
     Hit h;
     TraceWork w;
-    const bool hit = bvh_closest(nodes, tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, &h, w);
+    const bool hit = bvh_closest(nodes, nodes4, tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, &h, w);
     float* o = hits + 5 * (size_t)i;
     o[0] = hit ? h.t : b.w;
     o[1] = hit ? h.u : 0.f;
@@ -31,6 +32,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_closest(const BvhNode* __
 }
 
 __global__ void __launch_bounds__(kTraceBlock) k_trace_occluded(const BvhNode* __restrict__ nodes,
+                                                                const BvhNode4* __restrict__ nodes4,
                                                                 const BvhTri* __restrict__ tris,
                                                                 const float4* __restrict__ rays, uint8_t* occ,
                                                                 uint32_t n) {
@@ -39,7 +41,7 @@ __global__ void __launch_bounds__(kTraceBlock) k_trace_occluded(const BvhNode* _
     const float4 a = __ldg(&rays[2 * i]);
     const float4 b = __ldg(&rays[2 * i + 1]);
     TraceWork w;
-    occ[i] = bvh_occluded(nodes, tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, w) ? 1 : 0;
+    occ[i] = bvh_occluded(nodes, nodes4, tris, mk(a.x, a.y, a.z), mk(b.x, b.y, b.z), a.w, b.w, w) ? 1 : 0;
 }
 
 }  // namespace
@@ -48,13 +50,13 @@ cudaError_t launch_trace_closest(const DeviceBvh& bvh, const int* tri_attr, cons
                                  cudaStream_t s) {
     if (n == 0) return cudaSuccess;
     k_trace_closest<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, s>>>(
-        bvh.nodes, bvh.tris, tri_attr, (const float4*)rays, (float*)hits, n);
+        bvh.nodes, bvh.nodes4, bvh.tris, tri_attr, (const float4*)rays, (float*)hits, n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_trace_occluded(const DeviceBvh& bvh, const void* rays, uint8_t* occ, uint32_t n, cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    k_trace_occluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, s>>>(bvh.nodes, bvh.tris,
+    k_trace_occluded<<<(n + kTraceBlock - 1) / kTraceBlock, kTraceBlock, 0, s>>>(bvh.nodes, bvh.nodes4, bvh.tris,
                                                                                  (const float4*)rays, occ, n);
     return cudaGetLastError();
 }

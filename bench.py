@@ -370,11 +370,15 @@ def main():
 
     # Roofline of the dominant kernel. Algorithmic bytes come from a counting pass of the
     # plain renderer (1 spp, untimed): both renderers trace the same rays through the same
-    # BVH, so node visits (64 B) and triangle tests (48 B) per path are the same.
+    # tree (the 4-wide one: 128-B node records; the binary one: 64 B), so node visits and
+    # triangle tests (48 B) per path are the same.
     cw = frame(_abi.RENDER_PLAIN, count_work=1, spp_=1).stats
+    node_b = cw["node_bytes"]
+    if st.get("node_bytes", node_b) != node_b:
+        raise RuntimeError("the counting pass traversed another tree than the timed renderer")
     npaths = max(cw["paths"], 1)
-    closest_bpp = (cw["node_visits"] * 64 + cw["tri_tests"] * 48) / npaths
-    shadow_bpp = (cw["shadow_node_visits"] * 64 + cw["shadow_tri_tests"] * 48) / npaths
+    closest_bpp = (cw["node_visits"] * node_b + cw["tri_tests"] * 48) / npaths
+    shadow_bpp = (cw["shadow_node_visits"] * node_b + cw["shadow_tri_tests"] * 48) / npaths
     peak, peak_kind = peaks()
     if head == "plain":
         kname, kms, kbytes = "k_render_plain", kms_step, (closest_bpp + shadow_bpp) * paths_step
@@ -399,6 +403,7 @@ def main():
             "traffic": traffic, "peak_kind": peak_kind, "kernel": kname, "kernel_ms_per_step": kms,
             "algorithmic_bytes_per_step": kbytes,
             "closest_bytes_per_path": closest_bpp, "shadow_bytes_per_path": shadow_bpp,
+            "node_bytes": node_b,
             "closest_nodes_per_ray": cw["node_visits"] / max(cw["closest_rays"], 1),
             "shadow_nodes_per_ray": cw["shadow_node_visits"] / max(cw["shadow_rays"], 1),
             "stage_shares": shares}
@@ -413,11 +418,20 @@ def main():
         host_film = np.zeros((H, W, 4), np.float32)
         e2e_steps = max(1, min(args.steps, 2))
 
+        split = {"create": 0.0, "render": 0.0, "close": 0.0}
+
         def e2e_step():
+            t0 = time.perf_counter()
             sc2 = ab.Scene(ctx, data)
+            t1 = time.perf_counter()
             sc2.render(render_opts_for(data, modes[head], rank), out=host_film)
+            t2 = time.perf_counter()
             sc2.close()
+            t3 = time.perf_counter()
+            for k, v in (("create", t1 - t0), ("render", t2 - t1), ("close", t3 - t2)):
+                split[k] += v * 1000.0
         e2e_step()                                  # warm-up (untimed)
+        split = dict.fromkeys(split, 0.0)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -430,6 +444,7 @@ def main():
             dt = max_over_ranks(dt, device="cuda")
         e2e = {"value": world * paths_step / dt, "unit": "path samples/s", "h2d_bytes_per_step": int(desc_bytes),
                "d2h_bytes_per_step": int(host_film.nbytes), "ms_per_step": dt * 1000,
+               "split_ms": {k: v / e2e_steps for k, v in split.items()},
                "includes": "scene upload + device BVH build + render + film download"}
 
     adj = None if args.small else adjoint_ratio(ab, _abi, torch, ctx, stream)

@@ -264,7 +264,7 @@ typedef struct aur_render_stats {
     uint64_t closest_rays;  /* including camera rays */
     uint64_t shadow_rays;
     uint64_t paths;
-    uint64_t node_visits;   /* with count_work: 64-byte interior-node records fetched by closest-hit rays */
+    uint64_t node_visits;   /* with count_work: interior-node records fetched by closest-hit rays */
     uint64_t tri_tests;     /* with count_work: 48-byte triangle records tested by closest-hit rays */
     uint64_t launches;      /* kernels launched by the call */
     double kernel_ms;       /* device time of the render kernels */
@@ -272,7 +272,8 @@ typedef struct aur_render_stats {
     uint64_t shadow_tri_tests;
     double stage_ms[5];     /* wavefront: device time of regen, extend, sort, shade, shadow */
     int32_t wf_pool, wf_block, wf_sort;   /* wavefront configuration used (tuned or given) */
-    int32_t pad;
+    int32_t node_bytes;     /* bytes of one interior-node record of the tree traversed: 128 for the
+                               4-wide tree, 64 for the binary one */
 } aur_render_stats;
 
 AUR_API aur_status aur_render(aur_scene* scene, const aur_render_opts* opts, float* film_rgba, aur_render_stats* stats);
