@@ -34,9 +34,10 @@ namespace {
 enum : uint32_t { PS_EMPTY = 0, PS_ACTIVE = 1, PS_DONE = 2, PS_MASK = 3, PS_PENDING = 4 };
 // lane refill: a warp takes new rays once this many lanes are idle, and runs kRounds
 // traversal rounds (interior phase + leaf phase) between refill checks
-// (swept: refill 8-24 idle lanes x 1-3 rounds within 2%; 16 x 3 fastest)
+// (swept on the 4-wide tree: rounds 2 / 3 / 4 / 6 / 8 at 16 idle lanes 479.6 / 481.8 /
+// 488.1 / 472.7 / 463.8 M samples/s; refill 8-20 idle lanes within 0.5% at 4 rounds)
 constexpr int kRefill = 16;
-constexpr int kRounds = 3;
+constexpr int kRounds = 4;
 // resident 256-thread blocks per SM the traversal kernels are compiled for (register cap)
 #ifndef AUR_TRAV_MINB
 #define AUR_TRAV_MINB 4
