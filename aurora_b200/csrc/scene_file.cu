@@ -7,8 +7,8 @@
 //
 //   options    resolution, pixelsamples, lightsamples, mindepth, maxdepth, filename
 //   renderCam  fov (slope factor, camera.cpp:51-52), transforms (camera to world)
-//   shaders    texture2DShader, triplanarTextureShader (texture files in PFM; EXR needs
-//              OpenEXR, not in this build)
+//   shaders    texture2DShader, triplanarTextureShader (texture files in OpenEXR: scanline,
+//              NONE / RLE / ZIPS / ZIP; or PFM)
 //   materials  matteMaterial, kelemenMaterial, metalMaterial, glassMaterial; normalmap
 //   objects    geometry (OBJ triangles, optional Loop subdivision), light (square), envlight
 //
@@ -18,6 +18,8 @@
 // FP32 matrix arithmetic (core/transform.cpp:36-136, core/matrix4x4.cpp:49-150).
 #include "aur_capi_internal.h"
 #include "aur_host_math.h"
+#include "aur_image_io.h"
+#include <cctype>
 #include <cerrno>
 #include <cmath>
 #include <cstdio>
@@ -786,6 +788,21 @@ void read_pfm(const std::string& path, std::vector<float>* rgb, int* w, int* h) 
     *h = hh;
 }
 
+// A texture image: OpenEXR (what the reference reads) or PFM, by extension.
+void read_image(const std::string& path, std::vector<float>* rgb, int* w, int* h) {
+    const size_t dot = path.find_last_of('.');
+    std::string ext = dot == std::string::npos ? "" : path.substr(dot);
+    for (char& c : ext) c = (char)tolower((unsigned char)c);
+    if (ext == ".exr") {
+        std::string err;
+        const aur_status st = read_exr_rgb(path, rgb, w, h, &err);
+        if (st != AUR_OK) throw_load(st, err);
+        return;
+    }
+    if (ext != ".pfm") throw_load(AUR_ERR_UNSUPPORTED, "texture " + path + " is neither OpenEXR nor PFM");
+    read_pfm(path, rgb, w, h);
+}
+
 // ------------------------------------------------------------------ loader
 std::string dir_of(const std::string& p) {
     const size_t s = p.find_last_of('/');
@@ -847,14 +864,9 @@ struct Loader {
                 throw_load(AUR_ERR_PARSE, where + ": unknown shader type " + type);
             }
             const std::string path = resolve(dir, need_str(kv.second, "texturename", where));
-            const size_t dot = path.find_last_of('.');
-            const std::string ext = dot == std::string::npos ? "" : path.substr(dot);
-            if (ext != ".pfm" && ext != ".PFM")
-                throw_load(AUR_ERR_UNSUPPORTED, where + ": texture " + path + " is not a PFM file (EXR needs OpenEXR, "
-                                           "which this build does not include)");
             std::vector<float> rgb;
             int w = 0, h = 0;
-            read_pfm(path, &rgb, &w, &h);
+            read_image(path, &rgb, &w, &h);
             textures[kv.first] = (int)out.tex_dims.size() / 2;
             out.tex_dims.push_back(w);
             out.tex_dims.push_back(h);
@@ -1025,14 +1037,9 @@ struct Loader {
         const std::string map = need_str(o, "envmap", where);
         if (!map.empty()) {
             const std::string path = resolve(dir, map);
-            const size_t dot = path.find_last_of('.');
-            const std::string ext = dot == std::string::npos ? "" : path.substr(dot);
-            if (ext != ".pfm" && ext != ".PFM")
-                throw_load(AUR_ERR_UNSUPPORTED, where + ": env map " + path + " is not a PFM file (EXR needs OpenEXR, "
-                                                "which this build does not include)");
             std::vector<float> rgb;
             int w = 0, h = 0;
-            read_pfm(path, &rgb, &w, &h);
+            read_image(path, &rgb, &w, &h);
             l.tex = (int32_t)(out.tex_dims.size() / 2);
             out.tex_dims.push_back(w);
             out.tex_dims.push_back(h);

@@ -297,7 +297,9 @@ def test_triplanar_shader_normal_map_and_object_transform(tmp_path):
                                            "texturename": "t.pfm"}}}), _abi.ERR_PARSE),
     (lambda s: s["objects"].update({"e": {"type": "envlight"}}), _abi.ERR_PARSE),
     (lambda s: s["objects"].update({"e": {"type": "envlight", "transforms": [], "exposure": 0, "color": [1, 1, 1],
-                                          "envmap": "sky.exr"}}), _abi.ERR_UNSUPPORTED),
+                                          "envmap": "sky.exr"}}), _abi.ERR_IO),
+    (lambda s: s["objects"].update({"e": {"type": "envlight", "transforms": [], "exposure": 0, "color": [1, 1, 1],
+                                          "envmap": "sky.hdr"}}), _abi.ERR_UNSUPPORTED),
     (lambda s: s["objects"]["g"].update({"material": "nope"}), _abi.ERR_PARSE),
     (lambda s: s["objects"]["g"].update({"path": "missing.obj"}), _abi.ERR_IO),
     (lambda s: s["materials"]["m"].update({"color": "noshader"}), _abi.ERR_PARSE),
@@ -323,10 +325,11 @@ def test_json_syntax_error_names_the_line(tmp_path):
     assert e.value.status == _abi.ERR_PARSE and "line 4" in str(e.value)
 
 
-def test_exr_textures_are_refused(tmp_path):
+def test_other_image_formats_are_refused(tmp_path):
     v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
     write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
-    shaders = {"tex": {"attributetype": "color", "type": "texture2DShader", "texturename": "t.exr"}}
+    (tmp_path / "t.png").write_bytes(b"\x89PNG")
+    shaders = {"tex": {"attributetype": "color", "type": "texture2DShader", "texturename": "t.png"}}
     mats = {"m": {"type": "matteMaterial", "color": "tex"}}
     with pytest.raises(_abi.AuroraError) as e:
         scenes.load_scene_file(write_single(str(tmp_path), "q.obj", 0, materials=mats, shaders=shaders))
