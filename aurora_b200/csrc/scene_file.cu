@@ -311,6 +311,7 @@ float radians_f(float deg) { return (float)(deg * M_PI / 180.f); }   // math_uti
 Xform parse_transforms(const JValue* list, const std::string& where) {
     Xform t;
     if (!list) throw_load(AUR_ERR_PARSE, where + ": missing \"transforms\"");
+    if (list->kind == JValue::Obj && list->obj.empty()) return t;   // PyAurora writes an empty list as {}
     if (list->kind != JValue::Arr) throw_load(AUR_ERR_PARSE, where + ": \"transforms\" must be an array");
     for (const JValue& op : list->arr) {
         if (op.kind != JValue::Obj || op.obj.empty()) throw_load(AUR_ERR_PARSE, where + ": bad transform entry");
@@ -917,6 +918,8 @@ struct Loader {
                 color_attr(o, "transmitColor", m.diffuse, nullptr, where);
                 float_attr(o, "reflectance", &m.reflectance, nullptr, where);
                 float_attr(o, "ior", &m.ior, nullptr, where);
+            } else if (type == "carMaterial") {   // its construction is commented out in jsonParser.cpp:369-415
+                throw_load(AUR_ERR_UNSUPPORTED, where + ": carMaterial is disabled in the reference's parser");
             } else {
                 throw_load(AUR_ERR_PARSE, where + ": unknown material type " + type);
             }

@@ -63,3 +63,20 @@ def test_loop_subdivided_kelemen_sphere_file(ctx, kelemen_tables, oracle_lib, tm
     gpu, cpu, m2 = _render_both(ctx, kelemen_tables, oracle_lib, path, 8)
     _check(gpu, cpu, m2, 8)
     assert gpu[..., 3].mean() > 0.3   # the sphere and the ground fill the frame
+
+
+def test_scenegraph_render_writes_the_film(ctx, kelemen_tables, oracle_lib, tmp_path):
+    """PyAurora's render(scene) in-process: the scene file it writes renders like the oracle's
+    CPU render of the loaded arrays, and the film goes to the options' filename as half EXR."""
+    from aurora_b200 import scenes
+    from aurora_b200.scenegraph import core
+    from test_film_io import read_exr
+    from test_scenegraph import box_scene_graph
+    d = str(tmp_path)
+    path = os.path.join(d, "graph.json")
+    film = core.render(box_scene_graph(d, 48, 48, spp=8), path=path, ctx=ctx)
+    data, opts, _ = scenes.load_scene_file(path)
+    cpu, m2, _ = oracle_lib.OracleScene(data, kelemen_tables).render(8, opts.max_depth, opts.min_depth, opts.seed)
+    _check(film, cpu, m2, 8)
+    img, _ = read_exr(os.path.join(d, "box.exr"))
+    np.testing.assert_array_equal(img, film.astype(np.float16).astype(np.float32))
