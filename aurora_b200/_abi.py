@@ -87,6 +87,8 @@ class RenderStats(C.Structure):
 
 
 vp = C.c_void_p
+# aur_pass_fn: int32 (*)(void* user, const float* film, int32 samples_done)
+PASS_FN = C.CFUNCTYPE(C.c_int32, C.c_void_p, C.POINTER(C.c_float), C.c_int32)
 st = C.c_int
 pp = C.POINTER(C.c_void_p)
 
@@ -119,6 +121,7 @@ SIGNATURES = {
     "aur_scene_set_params": (st, [vp, vp, vp]),
     "aur_scene_get_params": (st, [vp, vp, vp]),
     "aur_render": (st, [vp, C.POINTER(RenderOpts), vp, C.POINTER(RenderStats)]),
+    "aur_render_progressive": (st, [vp, C.POINTER(RenderOpts), C.c_int32, vp, vp, vp, C.POINTER(RenderStats)]),
     "aur_render_f64": (st, [vp, C.POINTER(RenderOpts), vp, C.POINTER(RenderStats)]),
     "aur_render_fp64acc_noalloc": (st, [vp, C.POINTER(RenderOpts), vp, C.POINTER(RenderStats)]),
     "aur_render_batch": (st, [C.POINTER(C.c_void_p), C.POINTER(RenderOpts), C.c_uint32, C.POINTER(C.c_void_p),

@@ -188,6 +188,28 @@ class Scene:
         check(lib().aur_render(self.handle, C.byref(opts), _ptr(film), C.byref(s)), "aur_render")
         return RenderResult(film, _stats(s))
 
+    def render_progressive(self, opts: _abi.RenderOpts, pass_spp: int, on_pass=None, out=None) -> RenderResult:
+        """Renders opts.spp samples in passes of pass_spp; on_pass(film, samples_done) gets a
+        copy of the running mean (H, W, 4) after every pass and may return True to stop."""
+        film = out if out is not None else np.zeros((self.height, self.width, 4), np.float32)
+        s = _abi.RenderStats()
+        h, w = self.height, self.width
+        errors = []
+
+        def trampoline(_user, ptr, done):
+            try:
+                img = np.ctypeslib.as_array(ptr, shape=(h * w * 4,)).reshape(h, w, 4).copy()
+                return 1 if (on_pass(img, int(done)) if on_pass else False) else 0
+            except Exception as ex:                       # stop the render, re-raise below
+                errors.append(ex)
+                return 1
+        cb = _abi.PASS_FN(trampoline)
+        check(lib().aur_render_progressive(self.handle, C.byref(opts), int(pass_spp), C.cast(cb, C.c_void_p), None,
+                                           _ptr(film), C.byref(s)), "aur_render_progressive")
+        if errors:
+            raise errors[0]
+        return RenderResult(film, _stats(s))
+
     def render_f64(self, opts: _abi.RenderOpts) -> RenderResult:
         film = np.zeros((self.height, self.width, 4), np.float64)
         s = _abi.RenderStats()

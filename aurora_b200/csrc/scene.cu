@@ -410,7 +410,91 @@ static aur_status render_plain_impl(aur_scene* sc, const aur_render_opts* o, voi
     return AUR_OK;
 }
 
+namespace {
+
+// acc += pass mean * n (FP64 per channel); mean = acc / done
+__global__ void k_progressive(const float4* __restrict__ pass, double4* acc, float4* mean, uint32_t npix, double n,
+                              double done) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npix) return;
+    const float4 p = pass[i];
+    double4 a = acc[i];
+    a.x += (double)p.x * n; a.y += (double)p.y * n; a.z += (double)p.z * n; a.w += (double)p.w * n;
+    acc[i] = a;
+    mean[i] = make_float4((float)(a.x / done), (float)(a.y / done), (float)(a.z / done), (float)(a.w / done));
+}
+
+}  // namespace
+
 extern "C" {
+
+aur_status aur_render_progressive(aur_scene* sc, const aur_render_opts* o, int32_t pass_spp, aur_pass_fn on_pass,
+                                  void* user, float* film, aur_render_stats* stats) {
+    if (!sc || !o || !film) return fail(AUR_ERR_INVALID_ARG, "aur_render_progressive: NULL argument");
+    if (pass_spp < 1) return fail(AUR_ERR_INVALID_ARG, "aur_render_progressive: pass_spp must be >= 1");
+    if (o->spp < 1) return fail(AUR_ERR_INVALID_ARG, "aur_render_progressive: spp must be >= 1");
+    if (o->count_work || o->fp64_film) return fail(AUR_ERR_INVALID_ARG, "aur_render_progressive: count_work / fp64_film");
+    DeviceGuard g(sc->ctx->device);
+    cudaStream_t s = sc->ctx->stream;
+    const uint32_t npix = (uint32_t)sc->cam.w * (uint32_t)sc->cam.h;
+    float4 *pass = nullptr, *mean = nullptr;
+    double4* acc = nullptr;
+    std::vector<float> host;
+    cudaError_t e = cudaMallocAsync(&pass, sizeof(float4) * npix, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&mean, sizeof(float4) * npix, s);
+    if (e == cudaSuccess) e = cudaMallocAsync(&acc, sizeof(double4) * npix, s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(acc, 0, sizeof(double4) * npix, s);
+    auto release = [&]() {
+        if (pass) cudaFreeAsync(pass, s);
+        if (mean) cudaFreeAsync(mean, s);
+        if (acc) cudaFreeAsync(acc, s);
+        cudaStreamSynchronize(s);
+    };
+    if (e != cudaSuccess) { release(); return cuda_fail(e, "aur_render_progressive"); }
+    aur_render_stats total;
+    memset(&total, 0, sizeof(total));
+    int32_t done = 0;
+    aur_status st = AUR_OK;
+    while (done < o->spp) {
+        aur_render_opts po = *o;
+        po.spp = std::min(pass_spp, o->spp - done);
+        po.sample_offset = o->sample_offset + done;
+        aur_render_stats ps;
+        memset(&ps, 0, sizeof(ps));
+        st = aur_render(sc, &po, (float*)pass, &ps);
+        if (st != AUR_OK) break;
+        done += po.spp;
+        k_progressive<<<(npix + 255) / 256, 256, 0, s>>>(pass, acc, mean, npix, (double)po.spp, (double)done);
+        e = cudaGetLastError();
+        total.camera_rays += ps.camera_rays; total.closest_rays += ps.closest_rays;
+        total.shadow_rays += ps.shadow_rays; total.paths += ps.paths;
+        total.launches += ps.launches + 1; total.kernel_ms += ps.kernel_ms;
+        for (int k = 0; k < 5; ++k) total.stage_ms[k] += ps.stage_ms[k];
+        total.wf_pool = ps.wf_pool; total.wf_block = ps.wf_block; total.wf_sort = ps.wf_sort;
+        total.node_bytes = ps.node_bytes;
+        const bool last = done >= o->spp;
+        if (e == cudaSuccess && on_pass && !last) {
+            host.resize(4 * (size_t)npix);
+            e = cudaMemcpyAsync(host.data(), mean, sizeof(float4) * npix, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+            if (e == cudaSuccess && on_pass(user, host.data(), done) != 0) break;   // the caller stops here
+        }
+        if (e != cudaSuccess) break;
+    }
+    if (st == AUR_OK && e == cudaSuccess)
+        e = cudaMemcpyAsync(film, mean, sizeof(float4) * npix, cudaMemcpyDefault, s);
+    if (st == AUR_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (st == AUR_OK && e == cudaSuccess && on_pass && done >= o->spp) {
+        host.resize(4 * (size_t)npix);
+        e = cudaMemcpy(host.data(), mean, sizeof(float4) * npix, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess) on_pass(user, host.data(), done);
+    }
+    release();
+    if (st != AUR_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(e, "aur_render_progressive");
+    if (stats) *stats = total;
+    return AUR_OK;
+}
 
 aur_status aur_render(aur_scene* sc, const aur_render_opts* o, float* film, aur_render_stats* stats) {
     if (o && o->mode == AUR_RENDER_WAVEFRONT) return aur::render_wavefront(sc, o, film, stats);

@@ -111,11 +111,14 @@ def scene_json(scene):
     return root
 
 
-def render(scene, path=None, ctx=None, mode="wavefront", write_image=True):
+def render(scene, path=None, ctx=None, mode="wavefront", write_image=True, pass_spp=None, interval=1.0):
     """Writes the scene file (to `path`, default ./aurora_scene.json), loads it with the
     library's scene-file loader and renders it with the file's options on the GPU. The
     film is written, as OpenexrDisplay writes it (half RGBA), to the options' `filename`
-    (relative to the scene file's folder) when there is one. Returns the (H, W, 4) film."""
+    (relative to the scene file's folder) when there is one. With `pass_spp` the samples
+    are rendered in passes of that many and the image is also rewritten after a pass
+    whenever `interval` seconds have passed since the last write (the reference's
+    progressive display, renderer.cpp:240-262). Returns the (H, W, 4) film."""
     import numpy as np
     import aurora_b200 as ab
     from aurora_b200 import _abi
@@ -132,12 +135,23 @@ def render(scene, path=None, ctx=None, mode="wavefront", write_image=True):
             o = sc.file_opts
             o.mode = _abi.RENDER_WAVEFRONT if mode == "wavefront" else _abi.RENDER_PLAIN
             film = np.zeros((sc.height, sc.width, 4), np.float32)
-            sc.render(o, out=film)
+            out = root.get("options", {}).get("filename")
+            out = os.path.join(os.path.dirname(os.path.abspath(path)), out) if write_image and out else None
+            if pass_spp:
+                last = [time.monotonic()]
+
+                def on_pass(img, done):
+                    if out and time.monotonic() - last[0] >= interval:
+                        ab.write_film(out, img)
+                        last[0] = time.monotonic()
+                    return False
+                sc.render_progressive(o, pass_spp, on_pass, out=film)
+            else:
+                sc.render(o, out=film)
         finally:
             sc.close()
-        out = root.get("options", {}).get("filename")
-        if write_image and out:
-            ab.write_film(os.path.join(os.path.dirname(os.path.abspath(path)), out), film)
+        if out:
+            ab.write_film(out, film)
         return film
     finally:
         if own:

@@ -278,6 +278,19 @@ typedef struct aur_render_stats {
 
 AUR_API aur_status aur_render(aur_scene* scene, const aur_render_opts* opts, float* film_rgba, aur_render_stats* stats);
 
+/* Progressive rendering: Renderer::renderImage's pass loop with its periodic display
+ * (Aurora/src/frontend/renderer.cpp:240-262, OpenexrDisplay::draw). Renders opts->spp
+ * samples in passes of pass_spp (each pass the samples [offset + done, + pass_spp) of
+ * every pixel, as aur_render with sample_offset) and after every pass calls
+ * on_pass(user, film, samples_done) with the running mean film (width*height*4 floats of
+ * host memory owned by the library, valid during the call). A nonzero return stops after
+ * that pass; film_rgba (host or device) then holds the mean of the passes done. The film
+ * of a complete run equals aur_render's up to float rounding. */
+typedef int32_t (*aur_pass_fn)(void* user, const float* film_rgba, int32_t samples_done);
+AUR_API aur_status aur_render_progressive(aur_scene* scene, const aur_render_opts* opts, int32_t pass_spp,
+                                          aur_pass_fn on_pass, void* user, float* film_rgba,
+                                          aur_render_stats* stats);
+
 /* Plain renderer with FP64 accumulation and an FP64 film (width*height*4
  * doubles): the high-sample oracle images. */
 AUR_API aur_status aur_render_f64(aur_scene* scene, const aur_render_opts* opts, double* film_rgba, aur_render_stats* stats);

@@ -104,6 +104,30 @@ def test_texture_shaders_and_normal_maps(ctx, oracle_lib, kelemen_tables, mode):
     compare(g, mean, m2, 8)
 
 
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_progressive_passes(ctx, mode):
+    """aur_render_progressive: passes of 5 samples give the running mean after each pass and,
+    complete, the single render's film; a callback that returns True stops the render."""
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    data = scenes.box_scene(64, 64, spp=16)
+    r = data.render
+    scene = ab.Scene(ctx, data)
+    whole = scene.render(ab.render_opts(16, r["max_depth"], r["min_depth"], r["seed"], mode=mode)).film
+    seen = []
+    res = scene.render_progressive(ab.render_opts(16, r["max_depth"], r["min_depth"], r["seed"], mode=mode), 5,
+                                   lambda img, done: seen.append((done, img)) and False)
+    assert [d for d, _ in seen] == [5, 10, 15, 16] and res.stats["paths"] == 64 * 64 * 16
+    np.testing.assert_allclose(res.film, whole, rtol=1e-5, atol=1e-6)
+    np.testing.assert_array_equal(seen[-1][1], res.film)
+    ten = scene.render(ab.render_opts(10, r["max_depth"], r["min_depth"], r["seed"], mode=mode)).film
+    stopped = scene.render_progressive(ab.render_opts(16, r["max_depth"], r["min_depth"], r["seed"], mode=mode), 5,
+                                       lambda img, done: done >= 10)
+    np.testing.assert_allclose(stopped.film, ten, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(seen[1][1], ten, rtol=1e-5, atol=1e-6)
+    scene.close()
+
+
 def test_terrain_small(ctx, oracle_lib, kelemen_tables):
     """The large-scene generator at reduced size (roulette, 16 materials, 4 lights, depth 8)."""
     from aurora_b200 import scenes
