@@ -101,7 +101,7 @@ __device__ __forceinline__ bool bvh_trace(const BvhNode* __restrict__ nodes, con
 }
 
 // The same traversal over the 4-wide tree (one 128-byte record per node visit; hit
-// children nearest first for closest hits, slot order for any hit).
+// children nearest first).
 constexpr int kTraversalStack4Local = 96;
 template <bool kAnyHit>
 __device__ __forceinline__ bool bvh_trace4(const BvhNode4* __restrict__ nodes, const BvhTri* __restrict__ tris,
@@ -131,28 +131,16 @@ __device__ __forceinline__ bool bvh_trace4(const BvhNode4* __restrict__ nodes, c
             t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
             t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
             t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-            if (!kAnyHit) {
-                auto cx = [&](int i, int j) {
-                    if (t[j] < t[i]) { const float tt = t[i]; t[i] = t[j]; t[j] = tt; const int rr = r[i]; r[i] = r[j]; r[j] = rr; }
-                };
-                cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
-                if (t[0] != kMiss) {
-                    if (t[3] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[3];
-                    if (t[2] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[2];
-                    if (t[1] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[1];
-                    node = r[0];
-                    continue;
-                }
-            } else {
-                int next = -1;
-                bool any = false;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    if (t[c] == kMiss) continue;
-                    if (!any) { next = r[c]; any = true; }
-                    else if (sp < kTraversalStack4Local) stack[sp++] = r[c];
-                }
-                if (any) { node = next; continue; }
+            auto cx = [&](int i, int j) {   // nearest first, as the resumable traversal
+                if (t[j] < t[i]) { const float tt = t[i]; t[i] = t[j]; t[j] = tt; const int rr = r[i]; r[i] = r[j]; r[j] = rr; }
+            };
+            cx(0, 1); cx(2, 3); cx(0, 2); cx(1, 3); cx(1, 2);
+            if (t[0] != kMiss) {
+                if (t[3] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[3];
+                if (t[2] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[2];
+                if (t[1] != kMiss && sp < kTraversalStack4Local) stack[sp++] = r[1];
+                node = r[0];
+                continue;
             }
         } else {
             const int packed = ~node;
@@ -361,8 +349,8 @@ struct TraceState {
 
 // The same resumable while-while traversal over the 4-wide tree: a node visit loads
 // one 128-byte record, tests four boxes, and continues with the nearest hit child
-// while the other hit children go on the stack, farthest first. Boxes and the triangle test are the binary tree's, so the
-// closest hit equals it whenever the minimum is unique.
+// while the other hit children go on the stack, farthest first. Boxes and the triangle
+// test are the binary tree's, so the closest hit equals it whenever the minimum is unique.
 template <bool kAnyHit>
 struct TraceState4 {
     float3 o, d, id, ood;
