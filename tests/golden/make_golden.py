@@ -15,6 +15,12 @@ Contents (all generated from seeded inputs):
   box_mean, box_m2            box workload 16x16, 8 spp, depth 5: per-pixel mean (RGB, alpha)
                               and Welford sums
   box_dfilm, box_grad         a seeded dL/dfilm and the FP64 adjoint for it (materials x 4)
+  delta_sample_in / _out      256 mirror / transmission lobe samples (probe kind 0, lobes 2 and 4)
+  env_sample_in / _out        256 environment-map light samples of the sphere workload with a
+                              16x32 seeded env map (probe kind 6, the env light is light 2)
+  shade_point_in / _out       512 shading points of the texture-shader workload (probe kind 10:
+                              normal maps, triplanar colour and float shaders)
+  glass_mean, glass_m2        box workload 16x16 with glass boxes (lifted 0.01), 8 spp, depth 6
 """
 import os
 import sys
@@ -70,6 +76,39 @@ def make():
     dfilm[..., 3] = 0
     gm, _ = osc.adjoint(8, 5, 5, 1, dfilm, threads=1)
     out["box_dfilm"], out["box_grad"] = dfilm, gm
+
+    from aurora_b200 import _abi
+    m = 256
+    Nd = r.normal(size=(m, 3)); Nd /= np.linalg.norm(Nd, axis=1, keepdims=True)
+    Vd = r.normal(size=(m, 3)); Vd /= np.linalg.norm(Vd, axis=1, keepdims=True)
+    dl = np.where(r.uniform(size=m) < 0.5, 2, 4)
+    ior = np.where(dl == 4, r.uniform(1.1, 2.4, m), 0.0)
+    ds = np.concatenate([dl[:, None], r.uniform(0.1, 1, (m, 3)), ior[:, None], Vd, Nd, r.uniform(0, 1, (m, 2))],
+                        1).astype(np.float32)
+    out["delta_sample_in"] = ds
+    out["delta_sample_out"] = oracle.probe(0, ds)
+
+    envmap = np.random.default_rng(14).uniform(0.1, 3.0, (16, 32, 3)).astype(np.float32)
+    esc = scenes.sphere_scene(32, 32, env=dict(color=(1, 1, 1), exposure=0.5, texture=envmap))
+    P = r.uniform(-3, 3, (m, 3))
+    Ne = r.normal(size=(m, 3)); Ne /= np.linalg.norm(Ne, axis=1, keepdims=True)
+    es = np.concatenate([np.full((m, 1), 2.0), P, r.uniform(0, 1, (m, 2)), Ne], 1).astype(np.float32)
+    assert esc.lights[2].type == _abi.LIGHT_ENV
+    out["env_sample_in"] = es
+    out["env_sample_out"] = oracle.OracleScene(esc, tables).probe(6, es)
+
+    sys.path.insert(0, os.path.dirname(HERE))
+    from shade_points import hit_records
+    ssc = scenes.shader_scene(32, 32, sphere_level=2)
+    sp = hit_records(ssc, 512, 45)
+    out["shade_point_in"] = sp
+    out["shade_point_out"] = oracle.OracleScene(ssc, tables).probe(10, sp)
+
+    glass = dict(type_=_abi.MAT_GLASS, specular=(1.0, 1.0, 1.0), diffuse=(0.95, 0.9, 0.85), reflectance=0.04,
+                 ior=1.5)
+    gbox = scenes.box_scene(16, 16, spp=8, max_depth=6, box_mat=glass, lift=0.01)
+    gmean, gm2, _ = oracle.OracleScene(gbox, tables).render(8, 6, 6, 1, threads=1)
+    out["glass_mean"], out["glass_m2"] = gmean, gm2
     return out
 
 

@@ -27,3 +27,6 @@ def test_golden_sanity(golden):
     assert np.all((golden["rng_out"] >= 0) & (golden["rng_out"] < 1))
     assert np.all(golden["box_mean"][..., 3] == 1.0)        # the closed box covers every pixel
     assert np.any(golden["box_grad"][:3, :3] != 0)
+    assert set(np.unique(golden["delta_sample_in"][:, 0])) == {2.0, 4.0}
+    assert np.all(golden["env_sample_out"][:, 4] > 0)                  # env map pdfs
+    assert np.all(golden["glass_mean"][..., 3] == 1.0)
