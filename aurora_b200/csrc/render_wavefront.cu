@@ -828,14 +828,17 @@ static uint32_t fill_table(std::vector<BatchItem>& items, int s0, int chunk, flo
 }
 
 // Autotuner: times every candidate (pool size x block size x material sort) on the
-// same probe — the first `limit` work items of the real workload — and keeps the
-// fastest. Returns the chosen configuration.
+// same probe — the first `limit` work items of the real workload (at most 2^25) — and
+// keeps the fastest. Pools larger than twice the probe are not tried. (On the 1080p
+// depth-8 terrain, pools of 2^21 / 2^22 / 2^23 / 2^24 slots gave 475 / 491 / 504 / 509 M
+// samples/s: more paths in flight hide more of the traversal's fetch latency.)
+// Returns the chosen configuration.
 static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig* best_out) {
     cudaStream_t s = ctx->work_stream;
     size_t per_sample = 0;
     uint64_t total = 0;
     for (auto& it : items) { per_sample += (size_t)it.npix * sizeof(float4); total += (uint64_t)it.npix * it.p.spp; }
-    const uint32_t limit = (uint32_t)std::min<uint64_t>(total, 1ull << 24);
+    const uint32_t limit = (uint32_t)std::min<uint64_t>(total, 1ull << 25);
     int chunk = 1;   // samples buffer large enough for the probe's first `limit` items
     {
         uint32_t covered = 0;
@@ -846,7 +849,8 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
     if (e != cudaSuccess) return cuda_fail(e, "wavefront autotune");
     std::vector<WfScene> tab;
     fill_table(items, 0, chunk, samples, tab, std::max((int)items.size(), 64));
-    const uint32_t pools[3] = {1u << 20, 1u << 21, 1u << 22};
+    constexpr int kPools = 5;
+    const uint32_t pools[kPools] = {1u << 20, 1u << 21, 1u << 22, 1u << 23, 1u << 24};
     const int blocks[2] = {128, 256};
     double best = -1.0;
     WfConfig bestc;
@@ -854,7 +858,8 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
     bool warmed = false;
-    for (int pi = 0; pi < 3 && e == cudaSuccess; ++pi)
+    for (int pi = 0; pi < kPools && e == cudaSuccess; ++pi) {
+        if (pi > 0 && (uint64_t)pools[pi] > 2ull * limit) break;   // a pool that would stay mostly empty
         for (int bi = 0; bi < 2 && e == cudaSuccess; ++bi)
             for (int so = 0; so < 2 && e == cudaSuccess; ++so) {
                 WfConfig c;
@@ -879,6 +884,7 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
                 const double rate = ms > 0.f ? limit / ms : 0.0;
                 if (e == cudaSuccess && rate > best) { best = rate; bestc = c; }
             }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     cudaFreeAsync(samples, s);
