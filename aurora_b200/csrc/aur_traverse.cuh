@@ -40,6 +40,30 @@ __device__ __forceinline__ bool slab(float lox, float hix, float loy, float hiy,
     return tn <= tf;
 }
 
+// Slab test with the near and far planes already chosen by the ray direction's signs
+// (for a positive inverse direction the near plane is lo, else hi): the same entry and
+// exit distances as slab(), without the per-axis min/max.
+__device__ __forceinline__ bool slab_nf(float nx, float fx, float ny, float fy, float nz, float fz, float3 id,
+                                        float3 ood, float tmin, float tmax, float* tnear) {
+    const float tn = fmaxf(fmaxf(fmaf(nx, id.x, -ood.x), fmaf(ny, id.y, -ood.y)), fmaxf(fmaf(nz, id.z, -ood.z), tmin));
+    const float tf = fminf(fminf(fmaf(fx, id.x, -ood.x), fmaf(fy, id.y, -ood.y)), fminf(fmaf(fz, id.z, -ood.z), tmax));
+    *tnear = tn;
+    return tn <= tf;
+}
+
+// The four children's near and far planes of a 4-wide node: loads the lo or hi
+// float4 of each axis by the direction's sign (lox, hix, loy, hiy, loz, hiz order).
+struct Planes4 { float4 nx, fx, ny, fy, nz, fz; };
+__device__ __forceinline__ Planes4 load_planes4(const BvhNode4* q, float3 id) {
+    const float4* p = reinterpret_cast<const float4*>(q);
+    const int sx = id.x < 0.f, sy = id.y < 0.f, sz = id.z < 0.f;
+    Planes4 r;
+    r.nx = __ldg(p + sx); r.fx = __ldg(p + 1 - sx);
+    r.ny = __ldg(p + 2 + sy); r.fy = __ldg(p + 3 - sy);
+    r.nz = __ldg(p + 4 + sz); r.fz = __ldg(p + 5 - sz);
+    return r;
+}
+
 // kAnyHit=false: closest hit, returns true when hit->prim >= 0.
 // kAnyHit=true : returns true as soon as any triangle is hit in [mint, maxt].
 template <bool kAnyHit>
@@ -121,16 +145,15 @@ __device__ __forceinline__ bool bvh_trace4(const BvhNode4* __restrict__ nodes, c
         if (node >= 0) {
             ++work.nodes;
             const BvhNode4* q = nodes + node;
-            const float4 lx = __ldg(&q->lox), hx = __ldg(&q->hix), ly = __ldg(&q->loy), hy = __ldg(&q->hiy);
-            const float4 lz = __ldg(&q->loz), hz = __ldg(&q->hiz);
+            const Planes4 pl = load_planes4(q, id);
             const int4 rf = __ldg(&q->ref);
             float t[4];
             int r[4] = {rf.x, rf.y, rf.z, rf.w};
             float tc;
-            t[0] = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-            t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-            t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-            t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[0] = slab_nf(pl.nx.x, pl.fx.x, pl.ny.x, pl.fy.x, pl.nz.x, pl.fz.x, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[1] = slab_nf(pl.nx.y, pl.fx.y, pl.ny.y, pl.fy.y, pl.nz.y, pl.fz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[2] = slab_nf(pl.nx.z, pl.fx.z, pl.ny.z, pl.fy.z, pl.nz.z, pl.fz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+            t[3] = slab_nf(pl.nx.w, pl.fx.w, pl.ny.w, pl.fy.w, pl.nz.w, pl.fz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
             auto cx = [&](int i, int j) {   // nearest first, as the resumable traversal
                 if (t[j] < t[i]) { const float tt = t[i]; t[i] = t[j]; t[j] = tt; const int rr = r[i]; r[i] = r[j]; r[j] = rr; }
             };
@@ -376,17 +399,16 @@ struct TraceState4 {
 
     __device__ __forceinline__ void visit(const BvhNode4* __restrict__ nodes, LaneStack4& stack) {
         const BvhNode4* q = nodes + node;
-        const float4 lx = __ldg(&q->lox), hx = __ldg(&q->hix), ly = __ldg(&q->loy), hy = __ldg(&q->hiy);
-        const float4 lz = __ldg(&q->loz), hz = __ldg(&q->hiz);
+        const Planes4 pl = load_planes4(q, id);
         const int4 rf = __ldg(&q->ref);
         const float kMiss = __int_as_float(0x7f800000);
         float t[4];
         int r[4] = {rf.x, rf.y, rf.z, rf.w};
         float tc;
-        t[0] = slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-        t[1] = slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-        t[2] = slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
-        t[3] = slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[0] = slab_nf(pl.nx.x, pl.fx.x, pl.ny.x, pl.fy.x, pl.nz.x, pl.fz.x, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[1] = slab_nf(pl.nx.y, pl.fx.y, pl.ny.y, pl.fy.y, pl.nz.y, pl.fz.y, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[2] = slab_nf(pl.nx.z, pl.fx.z, pl.ny.z, pl.fy.z, pl.nz.z, pl.fz.z, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
+        t[3] = slab_nf(pl.nx.w, pl.fx.w, pl.ny.w, pl.fy.w, pl.nz.w, pl.fz.w, id, ood, box_tmin, box_tmax, &tc) ? tc : kMiss;
         // ascending by entry distance (misses last): a five-exchange network. Any-hit rays
         // take the same order (nearest first measured 1.6% faster than slot order for the
         // next-event rays, whose occluders tend to lie near the shading point).
