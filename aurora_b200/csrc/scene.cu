@@ -8,6 +8,7 @@
 #include "aur_host_math.h"
 #include <cmath>
 #include <cstring>
+#include <thread>
 
 using namespace aur;
 
@@ -219,9 +220,33 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
 
     DeviceGuard g(ctx->device);
     cudaStream_t s = ctx->stream;
+    // The per-corner normals and uvs (the largest inputs, 60 B per triangle) go up on
+    // their own stream and host thread while the BVH builds.
+    float *cn = nullptr, *cu = nullptr;
+    cudaError_t up_err = cudaSuccess;
+    cudaStream_t us = nullptr;
+    std::thread uploader;
+    if (cudaStreamCreateWithFlags(&us, cudaStreamNonBlocking) == cudaSuccess) {
+        uploader = std::thread([&]() {
+            DeviceGuard g2(ctx->device);
+            up_err = upload(&cn, d->corner_normals, 9 * (size_t)d->ntri, us);
+            if (up_err == cudaSuccess) up_err = upload(&cu, d->corner_uvs, 6 * (size_t)d->ntri, us);
+            cudaError_t se = cudaStreamSynchronize(us);
+            if (up_err == cudaSuccess) up_err = se;
+        });
+    } else {
+        cudaGetLastError();
+        us = nullptr;                // uploaded below on the context's stream
+    }
     aur_bvh* tmp = nullptr;
     aur_status st = aur_bvh_build(ctx, d->verts, d->nvert, d->tri_vidx, d->tri_attr, d->ntri, bvh_opts, &tmp);
-    if (st != AUR_OK) return st;
+    if (uploader.joinable()) uploader.join();
+    if (us) cudaStreamDestroy(us);
+    if (st != AUR_OK) {
+        if (cn) cudaFree(cn);
+        if (cu) cudaFree(cu);
+        return st;
+    }
     aur_scene* sc = new aur_scene();
     sc->ctx = ctx;
     sc->bvh = *tmp;
@@ -255,8 +280,14 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     cudaError_t e = cudaSuccess;
     for (const Material& m : mats)
         if (m.type == MAT_KELEMEN && e == cudaSuccess) e = ctx_kelemen_ensure(ctx, m.table);
-    if (e == cudaSuccess) e = upload(&sc->corner_n, d->corner_normals, 9 * (size_t)d->ntri, s);
-    if (e == cudaSuccess) e = upload(&sc->corner_uv, d->corner_uvs, 6 * (size_t)d->ntri, s);
+    if (us) {
+        sc->corner_n = cn;
+        sc->corner_uv = cu;
+        if (e == cudaSuccess) e = up_err;
+    } else {
+        if (e == cudaSuccess) e = upload(&sc->corner_n, d->corner_normals, 9 * (size_t)d->ntri, s);
+        if (e == cudaSuccess) e = upload(&sc->corner_uv, d->corner_uvs, 6 * (size_t)d->ntri, s);
+    }
     if (e == cudaSuccess) e = upload(&sc->attrs, attrs.data(), attrs.size(), s);
     if (e == cudaSuccess) e = upload(&sc->mats, mats.data(), mats.size(), s);
     if (e == cudaSuccess) e = upload(&sc->lights, lights.data(), lights.size(), s);
