@@ -75,7 +75,7 @@ class RenderOpts(C.Structure):
     _fields_ = [("spp", C.c_int32), ("sample_offset", C.c_int32), ("max_depth", C.c_int32),
                 ("min_depth", C.c_int32), ("seed", C.c_uint32), ("mode", C.c_int32), ("fp64_film", C.c_int32),
                 ("wf_pool", C.c_int32), ("wf_block", C.c_int32), ("wf_sort", C.c_int32),
-                ("count_work", C.c_int32)]
+                ("count_work", C.c_int32), ("light_samples", C.c_int32)]
 
 
 class RenderStats(C.Structure):

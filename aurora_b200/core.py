@@ -129,9 +129,9 @@ class RenderResult:
 
 
 def render_opts(spp, max_depth, min_depth, seed, mode=_abi.RENDER_PLAIN, sample_offset=0, fp64_film=0,
-                wf_pool=0, wf_block=0, wf_sort=-1, count_work=0) -> _abi.RenderOpts:
+                wf_pool=0, wf_block=0, wf_sort=-1, count_work=0, light_samples=0) -> _abi.RenderOpts:
     return _abi.RenderOpts(spp, sample_offset, max_depth, min_depth, seed, mode, fp64_film, wf_pool, wf_block,
-                           wf_sort, count_work)
+                           wf_sort, count_work, light_samples)
 
 
 def _stats(s: _abi.RenderStats) -> dict:

@@ -505,6 +505,7 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
     aur_status st = render_options(sc, o, &p);
     if (st != AUR_OK) return st;
     if (o->max_depth > kAdjMaxDepth) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: max_depth above 16");
+    if (p.light_samples > 1) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: light_samples > 1");
     if (o->mode != AUR_RENDER_PLAIN && o->mode != AUR_RENDER_WAVEFRONT)
         return fail(AUR_ERR_INVALID_ARG, "aur_render_adjoint: unknown mode");
     const bool wavefront = o->mode == AUR_RENDER_WAVEFRONT;

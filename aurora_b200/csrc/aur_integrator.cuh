@@ -28,6 +28,7 @@ struct PathParams {
     int max_depth, min_depth;
     int spp, sample_offset;
     uint32_t seed;
+    int light_samples;   // paths per camera sample after the first pass (1: one path)
 };
 
 struct RayCounts { uint32_t closest = 0, shadow = 0; TraceWork work, shadow_work; };
@@ -155,22 +156,12 @@ AUR_HD float3 firefly_clamp(float3 Lo) {
     return Lo;
 }
 
-// One camera path; returns the clamped radiance, sets *alpha to 1 on a camera hit.
+// The path from the camera ray's first hit `h` (ray `ray`, camera direction `cam_d`);
+// returns its firefly-filtered radiance.
 template <int kWidth>
-__device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathParams& p, int px, int py,
-                                                 const PathRng& rng, RayCounts& rc, float* alpha) {
-    RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
-    Hit h;
-    ++rc.closest;
-    *alpha = 0.f;
+__device__ __forceinline__ float3 path_from_hit(const DevScene& sc, const PathParams& p, RayF ray, Hit h,
+                                                const float3 cam_d, const PathRng& rng, RayCounts& rc) {
     float3 Lo = mk(0.f, 0.f, 0.f);
-    const float3 cam_d = ray.d;
-    if (!trace_closest<kWidth>(sc, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
-        if (sc.sh.nenv == 0) return Lo;
-        *alpha = 1.f;                       // environment seen directly: not firefly-filtered
-        return env_radiance(sc.sh, cam_d);
-    }
-    *alpha = 1.f;
     float3 T = mk(1.f, 1.f, 1.f);
     float cont = 1.f;
     bool matte_path = false;
@@ -201,6 +192,63 @@ __device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathP
         }
     }
     return firefly_clamp(Lo);
+}
+
+// One camera path; returns the clamped radiance, sets *alpha to 1 on a camera hit.
+template <int kWidth>
+__device__ __forceinline__ float3 integrate_path(const DevScene& sc, const PathParams& p, int px, int py,
+                                                 const PathRng& rng, RayCounts& rc, float* alpha) {
+    RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+    Hit h;
+    ++rc.closest;
+    *alpha = 0.f;
+    const float3 cam_d = ray.d;
+    if (!trace_closest<kWidth>(sc, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+        if (sc.sh.nenv == 0) return mk(0.f, 0.f, 0.f);
+        *alpha = 1.f;                       // environment seen directly: not firefly-filtered
+        return env_radiance(sc.sh, cam_d);
+    }
+    *alpha = 1.f;
+    return path_from_hit<kWidth>(sc, p, ray, h, cam_d, rng, rc);
+}
+
+// Integrator::integrateCameraSample(sample, numSamples) (integrator.cpp:152-300) in pass
+// `pass` (the sample index): the first pass traces one path per camera sample and later
+// passes p.light_samples paths from the camera ray's first hit (renderer.cpp:231-258
+// starts lightSamples at 1 and raises it after the first pass), each averaged in as
+// Lo / numSamples. Sub-path j of pass s draws from sample index s * L + j (L =
+// max(1, p.light_samples)); the camera ray from s * L. *paths = the paths traced.
+template <int kWidth>
+__device__ __forceinline__ float3 integrate_camera_sample(const DevScene& sc, const PathParams& p, int px, int py,
+                                                          uint32_t pixel, uint64_t key, int pass, RayCounts& rc,
+                                                          float* alpha, int* paths) {
+    const int lmax = p.light_samples > 1 ? p.light_samples : 1;
+    const int n = pass == 0 ? 1 : lmax;
+    PathRng rng;
+    rng.key = key;
+    rng.base = path_base(pixel, (uint32_t)(pass * lmax));
+    *paths = n;
+    RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+    Hit h;
+    ++rc.closest;
+    *alpha = 0.f;
+    const float3 cam_d = ray.d;
+    if (!trace_closest<kWidth>(sc, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+        if (sc.sh.nenv == 0) return mk(0.f, 0.f, 0.f);
+        *alpha = 1.f;                       // environment seen directly: not firefly-filtered
+        return env_radiance(sc.sh, cam_d);
+    }
+    *alpha = 1.f;
+    // one call site of the path (one copy of its code) for any number of sub-paths
+    float3 sum = mk(0.f, 0.f, 0.f);
+    for (int j = 0; j < n; ++j) {
+        PathRng rj = rng;
+        rj.base = path_base(pixel, (uint32_t)(pass * lmax + j));
+        const float3 v = path_from_hit<kWidth>(sc, p, ray, h, cam_d, rj, rc);
+        if (n == 1) sum = v;                 // Lo / 1.f: unchanged
+        else sum += cdiv(v, (float)n);
+    }
+    return sum;
 }
 
 }  // namespace aur

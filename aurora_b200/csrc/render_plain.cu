@@ -39,21 +39,21 @@ __global__ void __launch_bounds__(kPlainBlock) k_render_plain(DevScene sc, PathP
     uint32_t paths = 0;
     if (pixel < npix) {
         const int px = pixel % sc.cam.w, py = pixel / sc.cam.w;
-        PathRng rng;
-        rng.key = seed_key(p.seed);
+        const uint64_t key = seed_key(p.seed);
         Kahan3 acc;
         acc.init();
         double d[3] = {0.0, 0.0, 0.0};
         float alpha_sum = 0.f;
         for (int s = 0; s < p.spp; ++s) {
-            rng.base = path_base((uint32_t)pixel, (uint32_t)(p.sample_offset + s));
             float a;
-            const float3 L = integrate_path<kWidth>(sc, p, px, py, rng, rc, &a);
+            int n;
+            const float3 L = integrate_camera_sample<kWidth>(sc, p, px, py, (uint32_t)pixel, key, p.sample_offset + s,
+                                                             rc, &a, &n);
             if (kFp64) { d[0] += L.x; d[1] += L.y; d[2] += L.z; }
             else acc.add(L);
             alpha_sum += a;
+            paths += (uint32_t)n;
         }
-        paths = (uint32_t)p.spp;
         const float inv = 1.f / (float)p.spp;
         if (kFp64) {
             film64[4 * (size_t)pixel + 0] = d[0] / p.spp;

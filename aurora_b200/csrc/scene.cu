@@ -372,8 +372,14 @@ aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathPar
     if (!o) return fail(AUR_ERR_INVALID_ARG, "render: options are NULL");
     if (o->spp <= 0) return fail(AUR_ERR_INVALID_ARG, "render: spp must be positive");
     if (o->max_depth < 1 || o->max_depth > 400) return fail(AUR_ERR_INVALID_ARG, "render: max_depth must be 1..400");
-    if (o->sample_offset < 0 || (long long)o->sample_offset + o->spp > (1 << 20))
-        return fail(AUR_ERR_INVALID_ARG, "render: sample indices must stay below 2^20");
+    if (o->light_samples < 0 || o->light_samples > 4096)
+        return fail(AUR_ERR_INVALID_ARG, "render: light_samples must be 0..4096");
+    const long long lmax = o->light_samples > 1 ? o->light_samples : 1;
+    if (o->sample_offset < 0 || ((long long)o->sample_offset + o->spp) * lmax > (1 << 20))
+        return fail(AUR_ERR_INVALID_ARG, "render: sample indices (times light_samples) must stay below 2^20");
+    if (lmax > 1 && o->mode != AUR_RENDER_PLAIN)
+        return fail(AUR_ERR_UNSUPPORTED, "render: light_samples > 1 is rendered by the plain renderer (mode 0)");
+    p->light_samples = (int)lmax;
     p->max_depth = o->max_depth;
     p->min_depth = o->min_depth;
     p->spp = o->spp;

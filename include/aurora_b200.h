@@ -224,6 +224,12 @@ typedef struct aur_render_opts {
     int32_t wf_block;       /* wavefront block size, 0 = tuned/default */
     int32_t wf_sort;        /* wavefront material sort: -1 tuned, 0 off, 1 on */
     int32_t count_work;     /* also count BVH node visits / triangle tests (slower; for profiling) */
+    int32_t light_samples;  /* lightsamples (Integrator::integrateCameraSample's numSamples,
+                               integrator.cpp:152-300; renderer.cpp:231-258): 0 or 1 = one path per
+                               camera sample; L > 1 = the render's first pass (sample index 0)
+                               traces one path, every later pass L paths from the camera ray's
+                               first hit, each firefly-filtered, averaged. Plain renderer only;
+                               (sample_offset + spp) * L must stay below 2^20. */
 } aur_render_opts;
 
 /* ------------------------------------------------------------ scene files

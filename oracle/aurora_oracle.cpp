@@ -1025,20 +1025,10 @@ static Color integrateDirect(const Scene& sc, const LocalGeometry& lg, const Brd
 
 enum { CameraRay = 0, DiffuseRay = 1, SpecularRay = 2, MirrorRay = 3 };
 
-static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng, int maxDepth, int minDepth,
-                                   float* alpha, Counts& cnt) {
-    Ray ray = convertSample(sc, x, y, rng(0), rng(1));
-    const Vector camDir = ray.direction;
-    *alpha = 0;
-    ++cnt.closest;
-    int prim; float t, u, v;
-    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {   // camera miss: the environment lights (integrator.cpp:290-300)
-        Color env(0.f);
-        for (const Light& l : sc.lights)
-            if (l.type == AUR_LIGHT_ENV) { env += lightEval(sc, l, camDir); *alpha = 1.f; }
-        return env;
-    }
-    *alpha = 1.f;
+// One path from the camera ray's first hit (prim, t, u, v of `ray`); returns its
+// firefly-filtered radiance (integrator.cpp:169-285, one iteration of the numSamples loop).
+static Color pathFromHit(const Scene& sc, Ray ray, int prim, float t, float u, float v, const Vector& camDir,
+                         const Rng& rng, int maxDepth, int minDepth, Counts& cnt) {
     Color Lo(0.f);
     float continueProbability = 1.f;
     Color pathThroughput(1.f);
@@ -1087,6 +1077,42 @@ static Color integrateCameraSample(const Scene& sc, int x, int y, const Rng& rng
     if (!std::isfinite(Lo.r) || !std::isfinite(Lo.g) || !std::isfinite(Lo.b)) return Color(0.f);
     while (Lo.r > FIREFLY || Lo.g > FIREFLY || Lo.b > FIREFLY) Lo *= 0.2f;
     return Lo;
+}
+
+// Integrator::integrateCameraSample(sample, numSamples) (integrator.cpp:152-300) in pass
+// `pass`: the first pass of a render traces one path (renderer.cpp:231-258 starts
+// lightSamples at 1), later passes lightSamples paths from the camera ray's first hit,
+// each added as Lo / numSamples. Sub-path j draws from sample index pass * L + j
+// (L = max(1, lightSamples)); the camera ray from pass * L. *paths = paths traced.
+static Color integrateCameraSample(const Scene& sc, int x, int y, uint64_t key, uint32_t pixel, int pass,
+                                   int lightSamples, int maxDepth, int minDepth, float* alpha, Counts& cnt,
+                                   int* paths) {
+    const int lmax = lightSamples > 1 ? lightSamples : 1;
+    const int n = pass == 0 ? 1 : lmax;
+    *paths = n;
+    Rng rng; rng.key = key;
+    rng.base = ((uint64_t)pixel << 32) | ((uint64_t)(pass * lmax) << 12);
+    Ray ray = convertSample(sc, x, y, rng(0), rng(1));
+    const Vector camDir = ray.direction;
+    *alpha = 0;
+    ++cnt.closest;
+    int prim; float t, u, v;
+    if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {   // camera miss: the environment lights (integrator.cpp:290-300)
+        Color env(0.f);
+        for (const Light& l : sc.lights)
+            if (l.type == AUR_LIGHT_ENV) { env += lightEval(sc, l, camDir); *alpha = 1.f; }
+        return env;
+    }
+    *alpha = 1.f;
+    Color result(0.f);
+    for (int j = 0; j < n; ++j) {
+        Rng rj = rng;
+        rj.base = ((uint64_t)pixel << 32) | ((uint64_t)(pass * lmax + j) << 12);
+        const Color Lo = pathFromHit(sc, ray, prim, t, u, v, camDir, rj, maxDepth, minDepth, cnt);
+        if (n == 1) result = Lo;
+        else result += Lo / (float)n;
+    }
+    return result;
 }
 
 // ------------------------------------------------------------ adjoint restatement (FP64, forward mode)
@@ -1513,22 +1539,24 @@ int oracle_trace(void* h, const aur_ray* rays, uint32_t n, aur_hit* hits, int th
 // mean_rgba: w*h*4 doubles (RGB mean, alpha mean); m2_rgb: w*h*3 Welford sums of squared
 // deviations (may be NULL); counts[0..2] += closest rays, shadow rays, paths.
 int oracle_render(void* h, int spp, int sample_offset, int max_depth, int min_depth, uint32_t seed, int threads,
-                  int x0, int y0, int w, int hgt, double* mean_rgba, double* m2_rgb, uint64_t* counts) {
+                  int x0, int y0, int w, int hgt, double* mean_rgba, double* m2_rgb, uint64_t* counts,
+                  int light_samples) {
     const Scene& sc = *(Scene*)h;
     if (threads > 0) omp_set_num_threads(threads);
     const uint64_t key = key_of(seed);
-    uint64_t cl = 0, sh = 0;
-#pragma omp parallel for schedule(dynamic, 16) reduction(+ : cl, sh)
+    uint64_t cl = 0, sh = 0, np = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(+ : cl, sh, np)
     for (long long i = 0; i < (long long)w * hgt; ++i) {
         const int x = x0 + (int)(i % w), y = y0 + (int)(i / w);
         const uint32_t pixel = (uint32_t)y * (uint32_t)sc.width + (uint32_t)x;
         double mean[3] = {0, 0, 0}, m2[3] = {0, 0, 0}, a = 0;
         Counts cnt;
         for (int s = 0; s < spp; ++s) {
-            Rng rng; rng.key = key;
-            rng.base = ((uint64_t)pixel << 32) | ((uint64_t)(sample_offset + s) << 12);
             float alpha;
-            Color c = integrateCameraSample(sc, x, y, rng, max_depth, min_depth, &alpha, cnt);
+            int n;
+            Color c = integrateCameraSample(sc, x, y, key, pixel, sample_offset + s, light_samples, max_depth, min_depth,
+                                            &alpha, cnt, &n);
+            np += (uint64_t)n;
             const double v[3] = {c.r, c.g, c.b};
             for (int k = 0; k < 3; ++k) {            // Welford
                 const double dlt = v[k] - mean[k];
@@ -1542,7 +1570,7 @@ int oracle_render(void* h, int spp, int sample_offset, int max_depth, int min_de
         if (m2_rgb) for (int k = 0; k < 3; ++k) m2_rgb[3 * i + k] = m2[k];
         cl += cnt.closest; sh += cnt.shadow;
     }
-    if (counts) { counts[0] += cl; counts[1] += sh; counts[2] += (uint64_t)w * hgt * spp; }
+    if (counts) { counts[0] += cl; counts[1] += sh; counts[2] += np; }
     return 0;
 }
 

@@ -37,7 +37,7 @@ def lib() -> C.CDLL:
         L.oracle_scene_destroy.argtypes = [vp]
         L.oracle_scene_bvh_nodes.argtypes = [vp]
         L.oracle_trace.argtypes = [vp, vp, u32, vp, i32]
-        L.oracle_render.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp, vp]
+        L.oracle_render.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp, vp, i32]
         L.oracle_kelemen_table.argtypes = [C.c_float, i32, u32, vp, i32]
         L.oracle_shading_probe.argtypes = [vp, i32, vp, u32, vp, vp]
         L.oracle_adjoint.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp]
@@ -104,14 +104,19 @@ class OracleScene:
         lib().oracle_trace(self.h, rays.ctypes.data, rays.shape[0], hits.ctypes.data, threads)
         return hits
 
-    def render(self, spp, max_depth, min_depth, seed, crop=None, sample_offset=0, threads=0, want_m2=True):
+    def render(self, spp, max_depth, min_depth, seed, crop=None, sample_offset=0, threads=0, want_m2=True,
+               light_samples=1):
+        """Per-pixel mean (RGB, alpha) of spp passes over the crop, Welford sums of squares of
+        the pass values, and counts (closest rays, shadow rays, paths). light_samples > 1:
+        passes after the first trace that many paths from the camera ray's first hit."""
         W, H = self.data.width, self.data.height
         x0, y0, w, h = crop if crop is not None else (0, 0, W, H)
         mean = np.zeros((h, w, 4), np.float64)
         m2 = np.zeros((h, w, 3), np.float64) if want_m2 else None
         counts = np.zeros(3, np.uint64)
         lib().oracle_render(self.h, spp, sample_offset, max_depth, min_depth, seed, threads, x0, y0, w, h,
-                            mean.ctypes.data, None if m2 is None else m2.ctypes.data, counts.ctypes.data)
+                            mean.ctypes.data, None if m2 is None else m2.ctypes.data, counts.ctypes.data,
+                            int(light_samples))
         return mean, m2, counts
 
     def adjoint(self, spp, max_depth, min_depth, seed, dfilm, crop=None, sample_offset=0, threads=0):

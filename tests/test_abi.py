@@ -63,5 +63,5 @@ def test_record_layouts():
     from aurora_b200 import _abi
     assert C.sizeof(_abi.Ray) == 32
     assert C.sizeof(_abi.Hit) == 20
-    assert C.sizeof(_abi.RenderOpts) == 44
+    assert C.sizeof(_abi.RenderOpts) == 48
     assert C.sizeof(_abi.RenderStats) == 136

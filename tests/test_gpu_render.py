@@ -128,6 +128,25 @@ def test_progressive_passes(ctx, mode):
     scene.close()
 
 
+def test_light_samples(ctx, oracle_lib, kelemen_tables):
+    """light_samples 4: passes after the first trace four paths from the camera ray's first
+    hit, on the device as in the oracle; the wavefront renderer and the adjoint refuse it."""
+    import aurora_b200 as ab
+    from aurora_b200 import _abi, scenes
+    data = scenes.sphere_scene(48, 48)
+    scene = ab.Scene(ctx, data)
+    res = scene.render(ab.render_opts(6, 6, 6, 2, light_samples=4))
+    mean, m2, counts = oracle_lib.OracleScene(data, kelemen_tables).render(6, 6, 6, 2, light_samples=4)
+    compare(res.film, mean, m2, 6)
+    assert res.stats["paths"] == 48 * 48 * (1 + 5 * 4) == int(counts[2])
+    for call in (lambda: scene.render(ab.render_opts(6, 6, 6, 2, mode=_abi.RENDER_WAVEFRONT, light_samples=4)),
+                 lambda: scene.adjoint(ab.render_opts(6, 6, 6, 2, light_samples=4), np.zeros((48, 48, 4), np.float32))):
+        with pytest.raises(ab.AuroraError) as e:
+            call()
+        assert e.value.status == _abi.ERR_UNSUPPORTED
+    scene.close()
+
+
 def test_terrain_small(ctx, oracle_lib, kelemen_tables):
     """The large-scene generator at reduced size (roulette, 16 materials, 4 lights, depth 8)."""
     from aurora_b200 import scenes

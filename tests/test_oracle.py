@@ -305,3 +305,25 @@ def test_texture_shaders_and_normal_maps_known_answers(oracle_lib):
     assert all(np.count_nonzero(attr == a) > 300 for a in range(5))
     # the normal maps tilt the shading normal away from Ng
     assert np.mean(np.sum(got[:, :3] * got[:, 3:6], 1) < 0.999) > 0.3
+
+
+def test_light_samples_passes(oracle_lib):
+    """lightsamples (Integrator::integrateCameraSample's numSamples): the first pass traces one
+    path per camera sample, later passes L paths from the camera ray's first hit, averaged;
+    the estimate stays unbiased."""
+    from aurora_b200 import scenes
+    data = scenes.box_scene(16, 16, spp=8)
+    osc = oracle_lib.OracleScene(data, np.zeros((21, 64, 32), np.float32))
+    one, _, c1 = osc.render(1, 5, 5, 1, want_m2=False)
+    four, _, c4 = osc.render(1, 5, 5, 1, want_m2=False, light_samples=4)
+    np.testing.assert_array_equal(one, four)                 # pass 0: one path either way
+    _, _, c = osc.render(3, 5, 5, 1, want_m2=False, light_samples=4)
+    assert int(c[2]) == 16 * 16 * (1 + 4 + 4)
+    a, m2a, _ = osc.render(64, 5, 5, 3)
+    b, m2b, _ = osc.render(64, 5, 5, 3, light_samples=4)
+    np.testing.assert_array_equal(a[..., 3], b[..., 3])       # the same camera rays
+    sig = np.sqrt(m2a / 63 / 64 + m2b / 63 / 64)
+    assert np.mean(np.abs(a[..., :3] - b[..., :3]) <= 4 * sig + 1e-6) > 0.98
+    # L paths per pass lower the pass variance (the median pixel's: pixels that see the light
+    # keep the camera jitter's variance, which the sub-paths share)
+    assert np.median(m2b[..., :3]) < 0.6 * np.median(m2a[..., :3])

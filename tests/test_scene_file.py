@@ -325,6 +325,23 @@ def test_json_syntax_error_names_the_line(tmp_path):
     assert e.value.status == _abi.ERR_PARSE and "line 4" in str(e.value)
 
 
+def test_light_samples_option(tmp_path):
+    """The file's lightsamples reach the render options; several paths per camera sample
+    select the plain renderer."""
+    v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
+    write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
+    p = write_single(str(tmp_path), "q.obj", 0)
+    s = json.load(open(p))
+    s["options"]["lightsamples"] = 8
+    json.dump(s, open(p, "w"))
+    _, opts, info = scenes.load_scene_file(p)
+    assert opts.light_samples == 8 and opts.mode == _abi.RENDER_PLAIN and info["light_samples"] == 8
+    s["options"]["lightsamples"] = 1
+    json.dump(s, open(p, "w"))
+    _, opts, _ = scenes.load_scene_file(p)
+    assert opts.light_samples == 1 and opts.mode == _abi.RENDER_WAVEFRONT
+
+
 def test_other_image_formats_are_refused(tmp_path):
     v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
     write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
