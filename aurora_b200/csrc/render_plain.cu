@@ -30,7 +30,9 @@ __device__ __forceinline__ void add_counters(unsigned long long* counters, const
 // tree, on which this one-thread-per-path kernel is fastest (its code holds five
 // traversals; the 4-wide ones made it 30% slower); the counting pass can use either, to
 // count the work of the wavefront renderer's traversal.
-template <bool kFp64, bool kCount, int kWidth>
+// kMulti: light_samples > 1 (several paths per camera sample after the first pass); the
+// one-path form keeps the single-path loop, whose code is smaller and 6% faster.
+template <bool kFp64, bool kCount, int kWidth, bool kMulti>
 __global__ void __launch_bounds__(kPlainBlock) k_render_plain(DevScene sc, PathParams p, float4* film,
                                                               double* film64, unsigned long long* counters) {
     const int npix = sc.cam.w * sc.cam.h;
@@ -46,9 +48,16 @@ __global__ void __launch_bounds__(kPlainBlock) k_render_plain(DevScene sc, PathP
         float alpha_sum = 0.f;
         for (int s = 0; s < p.spp; ++s) {
             float a;
-            int n;
-            const float3 L = integrate_camera_sample<kWidth>(sc, p, px, py, (uint32_t)pixel, key, p.sample_offset + s,
-                                                             rc, &a, &n);
+            int n = 1;
+            float3 L;
+            if (kMulti) {
+                L = integrate_camera_sample<kWidth>(sc, p, px, py, (uint32_t)pixel, key, p.sample_offset + s, rc, &a, &n);
+            } else {
+                PathRng rng;
+                rng.key = key;
+                rng.base = path_base((uint32_t)pixel, (uint32_t)(p.sample_offset + s));
+                L = integrate_path<kWidth>(sc, p, px, py, rng, rc, &a);
+            }
             if (kFp64) { d[0] += L.x; d[1] += L.y; d[2] += L.z; }
             else acc.add(L);
             alpha_sum += a;
@@ -83,10 +92,15 @@ cudaError_t launch_render_plain(const DevScene& sc, const PathParams& p, float4*
                                 unsigned long long* counters, bool count_work, cudaStream_t s) {
     const int npix = sc.cam.w * sc.cam.h;
     const int grid = (npix + kPlainBlock - 1) / kPlainBlock;
-    if (film64) k_render_plain<true, false, 2><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
-    else if (count_work && sc.nodes4) k_render_plain<false, true, 4><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
-    else if (count_work) k_render_plain<false, true, 2><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
-    else k_render_plain<false, false, 2><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    const bool multi = p.light_samples > 1;
+    if (film64 && multi) k_render_plain<true, false, 2, true><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else if (film64) k_render_plain<true, false, 2, false><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else if (count_work && multi) return cudaErrorNotSupported;   // the counting pass counts one path per sample
+    else if (count_work && sc.nodes4)
+        k_render_plain<false, true, 4, false><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else if (count_work) k_render_plain<false, true, 2, false><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else if (multi) k_render_plain<false, false, 2, true><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
+    else k_render_plain<false, false, 2, false><<<grid, kPlainBlock, 0, s>>>(sc, p, film, film64, counters);
     return cudaGetLastError();
 }
 
