@@ -241,8 +241,8 @@ using LaneStack4 = LaneStackT<kTraversalStack4>;
 
 // Resumable traversal of one ray, for persistent kernels whose lanes take a new
 // ray as soon as theirs finishes (lane refill). Same visiting order, slack and
-// exact triangle test as bvh_trace; step() advances one interior node or one
-// leaf and returns true when the ray is finished.
+// exact triangle test as bvh_trace; round() advances every lane of a warp by one
+// while-while round and returns true when this lane's ray is finished.
 template <bool kAnyHit>
 struct TraceState {
     float3 o, d, id, ood;
@@ -326,49 +326,7 @@ struct TraceState {
         if (finished) return live;
         return leaf == kNone && node == kNone;
     }
-
-    __device__ __forceinline__ bool step(const BvhNode* __restrict__ nodes, const BvhTri* __restrict__ tris,
-                                         int* stack) {
-        if (node >= 0) {
-            const float4 a = __ldg(&nodes[node].a);
-            const float4 b = __ldg(&nodes[node].b);
-            const float4 c = __ldg(&nodes[node].c);
-            const float4 e = __ldg(&nodes[node].d);
-            float t0, t1;
-            const bool h0 = slab(a.x, a.y, a.z, a.w, c.x, c.y, id, ood, box_tmin, box_tmax, &t0);
-            const bool h1 = slab(b.x, b.y, b.z, b.w, c.z, c.w, id, ood, box_tmin, box_tmax, &t1);
-            const int r0 = __float_as_int(e.x), r1 = __float_as_int(e.y);
-            if (h0 && h1) {
-                const bool first0 = t0 <= t1;
-                if (sp < kTraversalStack) stack[sp++] = first0 ? r1 : r0;   // depth <= 63 is checked at build
-                node = first0 ? r0 : r1;
-                return false;
-            }
-            if (h0) { node = r0; return false; }
-            if (h1) { node = r1; return false; }
-        } else {
-            const int packed = ~node;
-            const int start = packed >> 5, end = start + (packed & 31);
-            for (int k = start; k < end; ++k) {
-                const float4 p = __ldg(&tris[k].p1);
-                const float4 e1 = __ldg(&tris[k].e1);
-                const float4 e2 = __ldg(&tris[k].e2);
-                float t, u, v;
-                if (tri_intersect(mk(p.x, p.y, p.z), mk(e1.x, e1.y, e1.z), mk(e2.x, e2.y, e2.z), o, d, mint, tbest,
-                                  &t, &u, &v)) {
-                    if (kAnyHit) { hit_any = true; return true; }
-                    tbest = t; bu = u; bv = v;
-                    best = __float_as_int(p.w);
-                    box_tmax = tbest * 1.00000095f;
-                }
-            }
-        }
-        if (sp == 0) return true;
-        node = stack[--sp];
-        return false;
-    }
 };
-
 
 // The same resumable while-while traversal over the 4-wide tree: a node visit loads
 // one 128-byte record, tests four boxes, and continues with the nearest hit child
