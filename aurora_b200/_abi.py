@@ -129,6 +129,7 @@ SIGNATURES = {
     "aur_render_adjoint": (st, [vp, C.POINTER(RenderOpts), vp, vp, vp, C.POINTER(RenderStats)]),
     "aur_kelemen_table": (st, [vp, C.c_float, vp]),
     "aur_shading_probe": (st, [vp, vp, C.c_int, vp, C.c_uint32, vp]),
+    "aur_measure_read_bandwidth": (st, [vp, C.c_uint64, C.c_int32, C.POINTER(C.c_double)]),
 }
 
 _lib = None

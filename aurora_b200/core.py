@@ -54,6 +54,13 @@ class Context:
         check(lib().aur_kelemen_table(self.handle, C.c_float(reflectance), _ptr(out)), "aur_kelemen_table")
         return out
 
+    def read_bandwidth(self, nbytes: int, reps: int) -> float:
+        """GB/s of `reps` reads of an `nbytes` device buffer (aur_measure_read_bandwidth)."""
+        out = C.c_double()
+        check(lib().aur_measure_read_bandwidth(self.handle, int(nbytes), int(reps), C.byref(out)),
+              "aur_measure_read_bandwidth")
+        return out.value
+
     def probe(self, kind: int, records: np.ndarray, scene: "Scene | None" = None) -> np.ndarray:
         records = np.ascontiguousarray(records, np.float32)
         n = records.shape[0]

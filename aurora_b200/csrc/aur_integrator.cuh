@@ -9,8 +9,11 @@
 // integrateDirectMIS (:56-98); throughput f*cos/pdf; a cumulative continue
 // probability and roulette when bounces > mindepth (:219-248); firefly clamp
 // (:278-281). The reference traces one more closest-hit ray after the last
-// shaded vertex whose hit is never shaded (it only matters for environment
-// lights, which are out of scope); that ray is skipped here.
+// shaded vertex; its hit is never shaded, and when it misses it adds the
+// environment lights if it is a mirror ray (:256-274). That ray is traced here
+// only when it can add something (a mirror ray in a scene with an environment
+// light), as an occlusion query over the same interval: whether it misses is
+// all that matters.
 #pragma once
 #include "aur_traverse.cuh"
 
@@ -178,7 +181,16 @@ __device__ __forceinline__ float3 path_from_hit(const DevScene& sc, const PathPa
         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
         if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
-        if (vtx + 1 >= p.max_depth) break;   // the reference's unshaded last ray
+        if (vtx + 1 >= p.max_depth) {
+            // the reference's unshaded last ray (integrator.cpp:256-274): an escaping mirror
+            // ray sees the environment along the camera ray's direction
+            if (kind == RAY_MIRROR && sc.sh.nenv) {
+                ++rc.closest;
+                if (!trace_occluded<kWidth>(sc, f.P, bs.dir, kRayBias, bs.maxt, rc.work))
+                    Lo += env_radiance(sc.sh, cam_d) * T;
+            }
+            break;
+        }
         ray.o = f.P;
         ray.d = bs.dir;
         ray.mint = kRayBias;

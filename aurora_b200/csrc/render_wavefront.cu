@@ -391,6 +391,9 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 if (S.sc.sh.nenv && (vtx == 0 || kind == RAY_MIRROR))
                     lo = shade_env_miss(w.id, w.tp, &S, slot, id, vtx, lo);
                 w.state[slot] = PS_DONE;
+            } else if (f_vtx(w.id[slot].w) >= w.scenes[w.id[slot].x].p.max_depth) {
+                // the reference's unshaded last ray hit something: the path ends
+                w.state[slot] = PS_DONE;
             } else {
                 const uint4 id = w.id[slot];
                 const WfScene& S = w.scenes[id.x];
@@ -477,8 +480,11 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 bool alive = false;
                 const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                                   rng.u(vertex_dim(vtx, kDimBrdf + 1)));
+                // after the last vertex the reference traces one more ray, which only an
+                // escaping mirror ray in a scene with an environment light turns into radiance
+                // (integrator.cpp:256-274): that ray is queued and its hit is not shaded
                 if (continue_path(brdf, bs, f.N, S.p.min_depth, rng, vtx, T, cont, kind, bounces) &&
-                    vtx + 1 < S.p.max_depth) {
+                    (vtx + 1 < S.p.max_depth || (kind == RAY_MIRROR && sc.sh.nenv))) {
                     alive = true;
                     w.ray_o[slot] = make_float4(f.P.x, f.P.y, f.P.z, kRayBias);
                     w.ray_d[slot] = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.maxt);

@@ -482,6 +482,20 @@ def sphere_scene(width=512, height=512, spp=64, max_depth=6, seed=2, ground_text
     return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))
 
 
+def mirror_quad_scene(width=16, height=16, spp=4, max_depth=1, seed=9, spec=(0.8, 0.6, 0.4),
+                      env=(0.5, 1.0, 2.0), exposure=0.0) -> SceneData:
+    """A 4x4 mirror quad (glassMaterial with reflectance 1: always SpecMirror) facing the camera at
+    distance 3, filling the view, under a constant environment light and nothing else. Every
+    camera ray hits the mirror and its reflection escapes, so every pixel is env * 2^exposure *
+    spec, at any max_depth (the last escape happens after the last shaded vertex at max_depth 1)."""
+    b = SceneBuilder(width, height, 0.4, name="mirror")
+    m = b.material(_abi.MAT_GLASS, specular=spec, diffuse=(1.0, 1.0, 1.0), reflectance=1.0, ior=1.5)
+    verts, faces = quad((-2, -2, -3), (2, -2, -3), (2, 2, -3), (-2, 2, -3))
+    b.mesh(verts, faces, m)
+    b.env_light(color=env, exposure=exposure)
+    return b.build(render=dict(spp=spp, max_depth=max_depth, min_depth=max_depth, seed=seed))
+
+
 def shader_scene(width=128, height=128, spp=16, max_depth=6, seed=3, tex_seed=11, sphere_level=4) -> SceneData:
     """Texture-shader workload: triplanar colour and roughness shaders, a normal-map texture and a
     constant normal map. A Kelemen sphere (triplanar diffuse, scale 0.5; triplanar roughness,

@@ -331,6 +331,14 @@ AUR_API aur_status aur_render_adjoint(aur_scene* scene, const aur_render_opts* o
  * rounded to half precision like the reference's EXR cache. */
 AUR_API aur_status aur_kelemen_table(aur_ctx* ctx, float reflectance, float* out_2048);
 
+/* ----------------------------------------------------------- measurement
+ * Read bandwidth of one memory level, the denominator of the traversal roofline
+ * (no reference counterpart): a device buffer of `bytes` (>= 1 MiB, allocated and
+ * freed by the call) is read `reps` times by a resident grid with 128-bit loads that
+ * bypass L1. Below the L2 size (126 MB on B200) the timed passes are served by the
+ * L2, above it by HBM. *gb_per_s = bytes * reps / device time (CUDA events). */
+AUR_API aur_status aur_measure_read_bandwidth(aur_ctx* ctx, uint64_t bytes, int32_t reps, double* gb_per_s);
+
 /* --------------------------------------------------------------- probes
  * Evaluates the device shading functions on n caller records (float arrays)
  * so that they can be compared value by value with a CPU restatement.

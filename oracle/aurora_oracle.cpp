@@ -15,7 +15,9 @@
 //     (b) a binned-SAH binary BVH for the timed baseline; both use the
 //     RenderableTriangle Moller-Trumbore test (renderableTriangle.cpp:68-98);
 //   * the film is an FP64 running sum (the reference keeps half precision);
-//   * the unshaded closest-hit ray after the last vertex is not traced.
+//   * the unshaded closest-hit ray after the last vertex (integrator.cpp:255-274)
+//     is traced only when its miss adds radiance (a mirror ray in a scene with an
+//     environment light); its hit is never shaded, so the radiance is the same.
 // The adjoint restatement (oracle_adjoint) has no reference counterpart: it is the
 // FP64 forward-mode derivative of this file's own estimator.
 // Parity pinning: the reference ships no tests, golden vectors or fixtures and
@@ -184,7 +186,16 @@ struct Scene {
     // CPU BVH (binned SAH) used by the timed baseline; brute force when empty
     std::vector<BvhNode> nodes;
     std::vector<int> order;
+    bool hasEnv = false;                    // an InfiniteAreaLight is among the lights
 };
+
+// Whether the ray after vertex trueBounces - 1 is traced: always below maxDepth; the one
+// after the last vertex only when an escaping mirror ray would see the environment
+// (integrator.cpp:255-274 traces it always, shades no hit, and adds the environment for
+// a mirror ray that misses).
+static bool traceNext(const Scene& sc, int trueBounces, int maxDepth, int rayType) {
+    return trueBounces < maxDepth || (rayType == 3 /* MirrorRay */ && sc.hasEnv);
+}
 
 // ------------------------------------------------------------ CPU BVH (baseline stand-in for Embree)
 struct BuildPrim { float lo[3], hi[3], c[3]; };
@@ -1061,7 +1072,7 @@ static Color pathFromHit(const Scene& sc, Ray ray, int prim, float t, float u, f
         cur.ray.origin = lg.P;
         ++trueBounces;
         if (!isMirrorType(brdf.type)) ++bounces;
-        if (trueBounces >= maxDepth) break;   // unshaded last ray skipped (no environment lights)
+        if (!traceNext(sc, trueBounces, maxDepth, rayType)) break;
         ray = cur.ray;
         ++cnt.closest;
         if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {
@@ -1286,7 +1297,7 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
             }
             cur.ray.origin = lg.P;
             ++trueBounces;
-            if (trueBounces >= maxDepth) break;
+            if (!traceNext(sc, trueBounces, maxDepth, rayType)) break;
             ray = cur.ray;
             if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {
                 if (rayType == MirrorRay) envMiss(sc, camDir, pathThroughput, dT, delta, Lo, contrib);
@@ -1323,7 +1334,7 @@ static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, i
         cur.ray.origin = lg.P;
         ++trueBounces;
         ++bounces;
-        if (trueBounces >= maxDepth) break;
+        if (!traceNext(sc, trueBounces, maxDepth, rayType)) break;
         ray = cur.ray;
         if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) {
                 if (rayType == MirrorRay) envMiss(sc, camDir, pathThroughput, dT, delta, Lo, contrib);
@@ -1382,6 +1393,7 @@ static Scene* makeScene(const aur_scene_desc* d, const float* albedo) {
             l.le = Color(ld.color[0], ld.color[1], ld.color[2]) * l.escale;
             invert4(l.m, l.minv);
             l.tex = ld.tex;                             // pdf normalisation once the texels are in
+            sc->hasEnv = true;
         } else if (ld.type == AUR_LIGHT_SQUARE) {
             l.xScale = ld.size_x; l.yScale = ld.size_y;
             Point p1 = xformPoint(l.m, Point(-l.xScale, -l.yScale, 0));

@@ -95,6 +95,23 @@ def test_adjoint_matches_fp64_oracle_under_an_env_map(ctx, kelemen_tables, oracl
 
 
 @pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_adjoint_matches_fp64_oracle_escape_after_last_vertex(ctx, kelemen_tables, oracle_lib, mode):
+    """Depth 2, a glass sphere on the textured ground under an env map: rays that leave the glass
+    after the last shaded vertex and escape add the map (integrator.cpp:255-274); their radiance
+    enters the gradients of the ground's texels and materials through the replayed throughput."""
+    from aurora_b200 import _abi, scenes
+    envmap = np.random.default_rng(16).uniform(0.05, 3.0, (32, 64, 3)).astype(np.float32)
+    tex = np.random.default_rng(7).uniform(0.2, 0.8, size=(64, 64, 3)).astype(np.float32)
+    glass = dict(type_=_abi.MAT_GLASS, specular=(1.0, 1.0, 1.0), diffuse=(0.9, 0.95, 1.0), reflectance=0.04, ior=1.5)
+    data = scenes.sphere_scene(256, 256, 64, 2, 2, ground_texture=tex, env=dict(color=(1, 1, 1), texture=envmap),
+                               sphere_mat=glass)
+    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (112, 150, 32, 32), 64, 2, 27, mode)
+    assert np.count_nonzero(ct) > 100
+    _compare(gm, cm, "materials (depth 2)")
+    _compare(gt, ct, "texels (depth 2)")
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
 def test_adjoint_matches_fp64_oracle_texture_shaders(ctx, kelemen_tables, oracle_lib, mode):
     """Triplanar diffuse shaders (each texel's gradient weighted by its blend weight) under
     normal maps: the ground, the sphere's diffuse lobe and the box."""

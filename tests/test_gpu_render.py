@@ -88,6 +88,40 @@ def test_environment_light(ctx, oracle_lib, kelemen_tables, mode, env):
 
 
 @pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+@pytest.mark.parametrize("max_depth", [1, 2])
+def test_mirror_escape_after_last_vertex(ctx, mode, max_depth):
+    """A mirror quad filling the view under a constant environment light: the reflection of every
+    camera ray escapes, after the last shaded vertex at max_depth 1 (integrator.cpp:255-274), so
+    every pixel is exactly env * 2^exposure * specular colour."""
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    spec, env, x = (0.8, 0.6, 0.4), (0.5, 1.0, 2.0), 1.0
+    data = scenes.mirror_quad_scene(max_depth=max_depth, spec=spec, env=env, exposure=x)
+    scene = ab.Scene(ctx, data)
+    res = scene.render(ab.render_opts(4, max_depth, max_depth, 9, mode=mode))
+    want = np.array(env, np.float64) * 2.0 ** x * np.array(spec, np.float64)
+    np.testing.assert_allclose(res.film[..., :3], np.broadcast_to(want, res.film[..., :3].shape), rtol=1e-6)
+    assert (res.film[..., 3] == 1.0).all()
+    assert res.stats["closest_rays"] == 2 * 16 * 16 * 4
+    scene.close()
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+@pytest.mark.parametrize("max_depth", [2, 3])
+def test_glass_under_env_map_shallow(ctx, oracle_lib, kelemen_tables, mode, max_depth):
+    """A glass sphere under an environment map at depth 2 and 3: many mirror and transmission
+    rays escape right after the last shaded vertex and add the map along the camera ray."""
+    from aurora_b200 import scenes
+    glass = dict(type_=5, specular=(1.0, 1.0, 1.0), diffuse=(0.9, 0.95, 1.0), reflectance=0.04, ior=1.5)
+    data = scenes.sphere_scene(96, 96, max_depth=max_depth, env=dict(color=(1, 1, 1), exposure=-1.0, texture=ENV_MAP),
+                               sphere_mat=glass)
+    g, mean, m2, counts, stats = render_both(ctx, oracle_lib, data, kelemen_tables, 16, mode=mode)
+    compare(g, mean, m2, 16)
+    if mode == 0:
+        assert stats["closest_rays"] == int(counts[0])
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
 def test_environment_map_with_kelemen(ctx, oracle_lib, kelemen_tables, mode):
     from aurora_b200 import scenes
     data = scenes.sphere_scene(96, 96, env=dict(color=(1, 1, 1), exposure=0.0, texture=ENV_MAP))

@@ -327,3 +327,20 @@ def test_light_samples_passes(oracle_lib):
     # L paths per pass lower the pass variance (the median pixel's: pixels that see the light
     # keep the camera jitter's variance, which the sub-paths share)
     assert np.median(m2b[..., :3]) < 0.6 * np.median(m2a[..., :3])
+
+
+@pytest.mark.parametrize("max_depth", [1, 2, 3])
+def test_mirror_escape_sees_environment(oracle_lib, max_depth):
+    """integrator.cpp:255-274: the ray after a mirror vertex that escapes adds the environment,
+    evaluated along the camera ray, times the throughput; this includes the ray after the LAST
+    shaded vertex (max_depth 1). A mirror quad (specular colour s) that fills the view under a
+    constant environment E * 2^x: every pixel is exactly E * 2^x * s, with alpha 1, and every
+    path traces two closest-hit rays (the camera ray and the escaping reflection)."""
+    from aurora_b200 import scenes
+    spec, env, x = (0.8, 0.6, 0.4), (0.5, 1.0, 2.0), 1.0
+    data = scenes.mirror_quad_scene(max_depth=max_depth, spec=spec, env=env, exposure=x)
+    mean, m2, counts = oracle_lib.OracleScene(data).render(4, max_depth, max_depth, 9)
+    want = np.array(env, np.float64) * 2.0 ** x * np.array(spec, np.float64)
+    np.testing.assert_allclose(mean[..., :3], np.broadcast_to(want, mean[..., :3].shape), rtol=1e-6)
+    assert (mean[..., 3] == 1.0).all()
+    assert int(counts[0]) == 2 * 16 * 16 * 4 and int(counts[1]) == 0

@@ -127,3 +127,23 @@ def _perturbed_texel_any(data, i, h):
     flat[i - sizes[k]] = flat[i - sizes[k]] + h
     d.textures = tex
     return d
+
+
+def test_oracle_adjoint_escape_after_last_vertex_matches_fd(oracle_lib):
+    """Depth 2, a glass sphere on a Lambert ground under a constant environment light: paths
+    camera -> ground -> glass whose mirror or transmission ray escapes after the LAST vertex
+    see the environment (integrator.cpp:255-274), so the ground albedo's gradient carries that
+    term. Checked against central differences of the oracle's renderer."""
+    from aurora_b200 import _abi, scenes
+    glass = dict(type_=_abi.MAT_GLASS, specular=(1.0, 1.0, 1.0), diffuse=(0.9, 0.95, 1.0), reflectance=0.04, ior=1.5)
+    data = scenes.sphere_scene(48, 48, 8, 2, 2, env=dict(color=(0.8, 0.9, 1.0)), sphere_mat=glass)
+    tables = np.zeros((21, 64, 32), np.float32)
+    w = np.random.default_rng(10).normal(size=(48, 48, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    crop, spp, seed = (8, 24, 32, 24), 8, 2
+    gm, _ = oracle_lib.OracleScene(data, tables).adjoint(spp, 2, 2, seed, w, crop=crop)
+    h = 1e-2
+    for c in range(3):
+        fd = (_loss(oracle_lib, _perturbed_material(data, 0, c, h), tables, w, spp, crop, seed) -
+              _loss(oracle_lib, _perturbed_material(data, 0, c, -h), tables, w, spp, crop, seed)) / (2 * h)
+        assert abs(gm[0, c] - fd) <= 0.01 * abs(fd) + 1e-6, (c, gm[0, c], fd)
