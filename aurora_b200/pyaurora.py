@@ -46,17 +46,24 @@ class AuroraRender(torch.autograd.Function):
     backward runs the path-replay adjoint with the same random numbers (wavefront mode: record
     pass on the wavefront engine + replay kernel; plain mode: one megakernel). options:
     spp, max_depth, min_depth, seed, mode ("wavefront" | "plain"), adjoint_spp.
+
+    The scene holds one set of parameters, and other renders of the same scene (a target
+    image, another forward) may change it between this forward and its backward. So the
+    forward keeps a copy of the parameters it rendered with; the backward replays the paths
+    under that copy and then puts back whatever the scene held when the backward began.
     """
 
     @staticmethod
     def forward(ctx, mat_params, texels, scene: Scene, options: dict):
         torch.cuda.synchronize()
-        scene.set_params(mat_params.detach().contiguous().float(),
-                         texels.detach().contiguous().float() if texels is not None and texels.numel() else None)
+        mp = mat_params.detach().contiguous().float().clone()
+        tx = texels.detach().contiguous().float().clone() if texels is not None and texels.numel() else None
+        scene.set_params(mp, tx)
         film = torch.empty((scene.height, scene.width, 4), dtype=torch.float32, device=mat_params.device)
         scene.render(_opts(options), out=film)
         ctx.scene, ctx.options = scene, options
-        ctx.has_tex = texels is not None and texels.numel() > 0
+        ctx.has_tex = tx is not None
+        ctx.fwd_params = (mp, tx)      # not save_for_backward: the caller may update the inputs in place
         return film
 
     @staticmethod
@@ -66,5 +73,11 @@ class AuroraRender(torch.autograd.Function):
         gm = torch.zeros((scene.nmat, 4), dtype=torch.float32, device=g.device)
         gt = torch.zeros(max(scene.ntexel, 1), dtype=torch.float32, device=g.device)
         torch.cuda.synchronize()
-        scene.adjoint(_opts(ctx.options, adjoint=True), g, gm, gt)
+        held_mp, held_tx = scene.get_params()
+        mp, tx = ctx.fwd_params
+        scene.set_params(mp, tx)
+        try:
+            scene.adjoint(_opts(ctx.options, adjoint=True), g, gm, gt)
+        finally:
+            scene.set_params(held_mp, held_tx if scene.ntexel else None)
         return gm, (gt[:scene.ntexel] if ctx.has_tex else None), None, None

@@ -305,12 +305,16 @@ AUR_API aur_status aur_render_f64(aur_scene* scene, const aur_render_opts* opts,
  * to float) that allocates no device memory. No counterpart in the reference.
  * For callers that cannot allocate: hosts that own all device memory through
  * their own allocator or a fixed budget. The film must be 16-byte aligned
- * device memory (width*height*4 floats); width*height must be <= 65536. The
- * scratch (FP64 accumulators, ray counters) is a static device array that every
- * GPU loading the library holds until exit (2 MiB). The first call on a device
- * looks up that array's address with the device current; make it before any
- * stream capture. All calls share the array: calls that overlap on the GPU race
- * and must be serialised by the caller. stats->kernel_ms is not measured (0). */
+ * device memory of the scene's device, or managed memory (width*height*4
+ * floats); width*height must be 1..65536. opts->fp64_film must be 1 and
+ * opts->count_work 0 (AUR_ERR_UNSUPPORTED otherwise); light_samples > 1 is
+ * supported. The scratch (FP64 accumulators, ray counters) is a static device
+ * array that every GPU loading the library holds until exit (2 MiB). Each call
+ * looks up that array's address with the scene's device current; the first
+ * call on a device may load the library's device code there, so make it
+ * before any stream capture. All calls share the array: calls that overlap on
+ * the GPU race and must be serialised by the caller. stats->kernel_ms is not
+ * measured (0). */
 AUR_API aur_status aur_render_fp64acc_noalloc(aur_scene* scene, const aur_render_opts* opts, float* film_device,
                                               aur_render_stats* stats);
 

@@ -105,6 +105,36 @@ def test_autograd_function(ctx):
     assert img.shape == (32, 32, 4)
 
 
+def test_autograd_backward_uses_the_forward_parameters(ctx):
+    """forward(A), forward(B), then the backward of A's image: the adjoint replays A's paths under
+    A's parameters (not B's, which the scene holds by then) and leaves the scene holding B."""
+    import torch
+    from aurora_b200.pyaurora import AuroraRender
+    data, scene, w = setup(ctx, res=32)
+    pa = data.material_params()
+    ta = data.texels()
+    rng = np.random.default_rng(3)
+    pb = np.clip(pa + rng.normal(0, 0.1, pa.shape), 0.05, 0.95).astype(np.float32)
+    tb = np.clip(ta + rng.normal(0, 0.1, ta.shape), 0.05, 0.95).astype(np.float32)
+    params_a = torch.tensor(pa, device="cuda", requires_grad=True)
+    texels_a = torch.tensor(ta, device="cuda", requires_grad=True)
+    opts = dict(spp=8, max_depth=6, seed=2)
+    img_a = AuroraRender.apply(params_a, texels_a, scene, opts)
+    with torch.no_grad():
+        AuroraRender.apply(torch.tensor(pb, device="cuda"), torch.tensor(tb, device="cuda"), scene, opts)
+    (img_a * torch.tensor(w, device="cuda")).sum().backward()
+    held_p, held_t = scene.get_params()
+    np.testing.assert_array_equal(held_p, pb)
+    np.testing.assert_array_equal(held_t, tb)
+    scene.set_params(pa, ta)
+    gm, gt, _ = adjoint(scene, w, 8, mode=1)
+    np.testing.assert_allclose(params_a.grad.cpu().numpy(), gm, rtol=1e-5, atol=1e-6)
+    np.testing.assert_allclose(texels_a.grad.cpu().numpy(), gt, rtol=1e-5, atol=1e-6)
+    scene.set_params(pb, tb)
+    gm_b, _, _ = adjoint(scene, w, 8, mode=1)
+    assert not np.allclose(gm_b, gm, rtol=1e-3)      # B's gradients differ: the check has teeth
+
+
 @pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
 def test_adjoint_is_deterministic(ctx, mode):
     data, scene, w = setup(ctx, res=32)
