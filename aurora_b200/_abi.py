@@ -43,6 +43,11 @@ class Hit(C.Structure):
     _fields_ = [("t", C.c_float), ("u", C.c_float), ("v", C.c_float), ("prim", C.c_int32), ("attr", C.c_int32)]
 
 
+class Isect(C.Structure):
+    _fields_ = [("t", C.c_float), ("u", C.c_float), ("v", C.c_float), ("prim", C.c_int32), ("attr", C.c_int32),
+                ("hitP", f3), ("hitN", f3), ("st", C.c_float * 2), ("bar", f3)]
+
+
 class BvhOpts(C.Structure):
     _fields_ = [("max_leaf", C.c_int32), ("cost_traverse", C.c_float), ("cost_intersect", C.c_float),
                 ("ploc_radius", C.c_int32)]
@@ -106,6 +111,8 @@ SIGNATURES = {
     "aur_bvh_info": (st, [vp, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32), C.POINTER(C.c_float)]),
     "aur_trace_closest": (st, [vp, vp, vp, C.c_uint32]),
     "aur_trace_occluded": (st, [vp, vp, vp, C.c_uint32]),
+    "aur_bvh_set_shading": (st, [vp, vp, vp]),
+    "aur_bvh_intersect": (st, [vp, vp, vp, C.c_uint32]),
     "aur_scene_create": (st, [vp, C.POINTER(SceneDesc), C.POINTER(BvhOpts), pp]),
     "aur_scene_load_json": (st, [vp, C.c_char_p, C.POINTER(BvhOpts), pp, C.POINTER(RenderOpts)]),
     "aur_scene_file_read": (st, [C.c_char_p, pp]),

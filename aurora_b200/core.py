@@ -76,6 +76,9 @@ def bvh_opts(max_leaf=0, cost_traverse=0.0, cost_intersect=0.0, ploc_radius=0) -
 
 
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<i4"), ("attr", "<i4")])
+# aur_isect: EmbreeAccelerator::intersect's full record
+ISECT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<i4"), ("attr", "<i4"),
+                        ("hitP", "<f4", 3), ("hitN", "<f4", 3), ("st", "<f4", 2), ("bar", "<f4", 3)])
 
 
 class Bvh:
@@ -127,6 +130,20 @@ class Bvh:
         occ = np.zeros(rays.shape[0], np.uint8)
         check(lib().aur_trace_occluded(self.handle, _ptr(rays), _ptr(occ), rays.shape[0]), "aur_trace_occluded")
         return occ
+
+    def set_shading(self, corner_normals, corner_uvs=None):
+        """Per-corner normals (ntri, 9) and uvs (ntri, 6) that intersect() interpolates."""
+        n = np.ascontiguousarray(corner_normals, np.float32)
+        uv = None if corner_uvs is None else np.ascontiguousarray(corner_uvs, np.float32)
+        check(lib().aur_bvh_set_shading(self.handle, _ptr(n), _ptr(uv)), "aur_bvh_set_shading")
+
+    def intersect(self, rays: np.ndarray):
+        """EmbreeAccelerator::intersect for (n, 8) rays: (ISECT_DTYPE records, the rays with maxt
+        shrunk to t where they hit)."""
+        rays = np.array(rays, np.float32, copy=True, order="C")
+        out = np.zeros(rays.shape[0], ISECT_DTYPE)
+        check(lib().aur_bvh_intersect(self.handle, _ptr(rays), _ptr(out), rays.shape[0]), "aur_bvh_intersect")
+        return out, rays
 
 
 @dataclass

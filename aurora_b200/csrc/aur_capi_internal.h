@@ -29,6 +29,11 @@ struct aur_bvh {
     int* tri_attr = nullptr;                   // device, per original triangle id
     bool owns_attr = false;
     bool owned_by_scene = false;
+    // per-corner normals (9 floats) and uvs (6 floats) per triangle for aur_bvh_intersect:
+    // the scene's arrays for a scene's BVH, else uploaded by aur_bvh_set_shading (owned)
+    float* corner_n = nullptr;
+    float* corner_uv = nullptr;
+    bool owns_shading = false;
 };
 
 struct aur_scene {
@@ -53,6 +58,8 @@ struct aur_scene {
     int wf_pool = 0, wf_block = 0, wf_sort = 0;
     aur::DevScene dev() const;
 };
+
+#define CUDA_TRY(x, where) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return aur::cuda_fail(e_, where); } while (0)
 
 namespace aur {
 

@@ -105,7 +105,6 @@ int kelemen_index(float reflectance) {
 }
 }  // namespace aur
 
-#define CUDA_TRY(x, where) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return cuda_fail(e_, where); } while (0)
 
 extern "C" {
 
@@ -270,6 +269,8 @@ aur_status aur_bvh_destroy(aur_bvh* b) {
     DeviceGuard g(b->ctx->device);
     bvh_free_device(&b->bvh, b->ctx->stream);
     if (b->owns_attr && b->tri_attr) cudaFreeAsync(b->tri_attr, b->ctx->stream);
+    if (b->owns_shading && b->corner_n) cudaFreeAsync(b->corner_n, b->ctx->stream);
+    if (b->owns_shading && b->corner_uv) cudaFreeAsync(b->corner_uv, b->ctx->stream);
     cudaStreamSynchronize(b->ctx->stream);
     delete b;
     return AUR_OK;

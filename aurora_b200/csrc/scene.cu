@@ -12,7 +12,6 @@
 
 using namespace aur;
 
-#define CUDA_TRY(x, where) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return cuda_fail(e_, where); } while (0)
 
 namespace aur {
 
@@ -296,6 +295,8 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     if (e == cudaSuccess) e = upload(&sc->attr_c2o, c2o.data(), c2o.size(), s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) { scene_free(sc); return cuda_fail(e, "aur_scene_create"); }
+    sc->bvh.corner_n = sc->corner_n;       // aur_bvh_intersect on aur_scene_bvh reads the scene's arrays
+    sc->bvh.corner_uv = sc->corner_uv;
     *out = sc;
     return AUR_OK;
 }

@@ -105,6 +105,30 @@ AUR_API aur_status aur_trace_closest(aur_bvh* bvh, const aur_ray* rays, aur_hit*
  * [mint, maxt] — EmbreeAccelerator::intersectBinary (embreeAccelerator.cpp:96-100). */
 AUR_API aur_status aur_trace_occluded(aur_bvh* bvh, const aur_ray* rays, uint8_t* occluded, uint32_t n);
 
+/* The full hit record of EmbreeAccelerator::intersect (embreeAccelerator.cpp:41-91):
+ * Intersection::hitP / hitN / attributesIndex and its ShadingGeometry P, Ng, st,
+ * triangleIndex, barCoords. 64 bytes. */
+typedef struct aur_isect {
+    float t, u, v;         /* distance; barycentrics u (vertex 1), v (vertex 2) */
+    int32_t prim;          /* shdGeo.triangleIndex (id1); -1 on a miss */
+    int32_t attr;          /* attributesIndex (id0); -1 on a miss */
+    float hitP[3];         /* hitP = shdGeo.P = org + dir * t */
+    float hitN[3];         /* hitN = shdGeo.Ng: normalize(w n0 + u n1 + v n2) with w = 1 - u - v,
+                              negated first when it points along dir (face-forward) */
+    float st[2];           /* shdGeo.st = w st0 + u st1 + v st2 (0 without uvs) */
+    float bar[3];          /* shdGeo.barCoords = (u, v, w) */
+} aur_isect;
+
+/* The per-corner normals (ntri x 9 floats, EmbreeMesh::normals[3 * triangle + k]) and uvs
+ * (ntri x 6, EmbreeMesh::uvs, may be NULL) that aur_bvh_intersect interpolates
+ * (geometry/embreeMesh.h:62-63: the mesh keeps them after the build). Copied to the
+ * device; refused for a scene's BVH, which uses the scene's arrays. */
+AUR_API aur_status aur_bvh_set_shading(aur_bvh* bvh, const float* corner_normals, const float* corner_uvs);
+/* EmbreeAccelerator::intersect (embreeAccelerator.cpp:41-91) for n rays: the closest hit
+ * and its post-process into isects[i]; on a hit rays[i].maxt becomes t (the reference
+ * shrinks ray->maxt), so rays is read and written (host or device memory). */
+AUR_API aur_status aur_bvh_intersect(aur_bvh* bvh, aur_ray* rays, aur_isect* isects, uint32_t n);
+
 /* ------------------------------------------------------------------ scene
  * Materials: Aurora/src/shading/materials/{matte,kelemen,metal,constant}Material.cpp.
  * COOKTORRANCE is one Cook-Torrance (Beckmann) lobe with colour `specular`

@@ -1547,6 +1547,36 @@ int oracle_trace(void* h, const aur_ray* rays, uint32_t n, aur_hit* hits, int th
     return 0;
 }
 
+// EmbreeAccelerator::intersect's post-process (embreeAccelerator.cpp:49-90) of given hits:
+// out[8 i ..] = hitP xyz, hitN xyz (face-forwarded, normalised), st; zeros for a miss.
+int oracle_isect_post(void* h, const aur_ray* rays, const aur_hit* hits, uint32_t n, float* out) {
+    const Scene& sc = *(Scene*)h;
+    for (uint32_t r = 0; r < n; ++r) {
+        float* o = out + 8 * (size_t)r;
+        for (int k = 0; k < 8; ++k) o[k] = 0.f;
+        if (hits[r].prim < 0) continue;
+        const int prim = hits[r].prim;
+        const float u = hits[r].u, v = hits[r].v, t = hits[r].t;
+        const Point org(rays[r].org[0], rays[r].org[1], rays[r].org[2]);
+        const Vector dir(rays[r].dir[0], rays[r].dir[1], rays[r].dir[2]);
+        float w = 1. - u - v;
+        const float* nn = &sc.cornerN[(size_t)prim * 9];
+        Vector norm(w * nn[0] + u * nn[3] + v * nn[6], w * nn[1] + u * nn[4] + v * nn[7],
+                    w * nn[2] + u * nn[5] + v * nn[8]);
+        if (dot(norm, dir) > 0.) norm = norm * -1;
+        const Vector hitN = normalize(norm);
+        const Point hitP = org + (dir * t);
+        o[0] = hitP.x; o[1] = hitP.y; o[2] = hitP.z;
+        o[3] = hitN.x; o[4] = hitN.y; o[5] = hitN.z;
+        if (!sc.cornerUV.empty()) {
+            const float* uv = &sc.cornerUV[(size_t)prim * 6];
+            o[6] = w * uv[0] + u * uv[2] + v * uv[4];
+            o[7] = w * uv[1] + u * uv[3] + v * uv[5];
+        }
+    }
+    return 0;
+}
+
 // Renders pixels [x0, x0+w) x [y0, y0+h) of the full image with spp camera paths each.
 // mean_rgba: w*h*4 doubles (RGB mean, alpha mean); m2_rgb: w*h*3 Welford sums of squared
 // deviations (may be NULL); counts[0..2] += closest rays, shadow rays, paths.

@@ -37,6 +37,7 @@ def lib() -> C.CDLL:
         L.oracle_scene_destroy.argtypes = [vp]
         L.oracle_scene_bvh_nodes.argtypes = [vp]
         L.oracle_trace.argtypes = [vp, vp, u32, vp, i32]
+        L.oracle_isect_post.argtypes = [vp, vp, vp, u32, vp]
         L.oracle_render.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp, vp, i32]
         L.oracle_kelemen_table.argtypes = [C.c_float, i32, u32, vp, i32]
         L.oracle_shading_probe.argtypes = [vp, i32, vp, u32, vp, vp]
@@ -103,6 +104,15 @@ class OracleScene:
         hits = np.zeros(rays.shape[0], HIT_DTYPE)
         lib().oracle_trace(self.h, rays.ctypes.data, rays.shape[0], hits.ctypes.data, threads)
         return hits
+
+    def isect_post(self, rays, hits):
+        """EmbreeAccelerator::intersect's post-process of `hits` (HIT_DTYPE): (n, 8) float32 rows of
+        hitP xyz, hitN xyz, st (zeros for misses)."""
+        rays = np.ascontiguousarray(rays, np.float32)
+        hits = np.ascontiguousarray(hits, HIT_DTYPE)
+        out = np.zeros((rays.shape[0], 8), np.float32)
+        lib().oracle_isect_post(self.h, rays.ctypes.data, hits.ctypes.data, rays.shape[0], out.ctypes.data)
+        return out
 
     def render(self, spp, max_depth, min_depth, seed, crop=None, sample_offset=0, threads=0, want_m2=True,
                light_samples=1):
