@@ -282,13 +282,15 @@ __device__ __forceinline__ ParamRef param_of(const ShadeScene& sh, int mat_id, c
 }
 
 // Pass 2 of one camera path: re-shades the recorded vertices rec[0, nv) (no ray
-// tracing) and accumulates dL/dtheta with delta = dLoss/dpixel / spp. Lo is the path's
-// unclamped radiance from pass 1.
+// tracing) and accumulates dL/dtheta with delta = dLoss/dpixel / spp (/ n for one of the
+// n paths of a camera sample with light samples). Lo is the path's unclamped radiance
+// from pass 1; cam_rng draws the camera ray (the path's own rng but for light samples,
+// whose paths share their sample's camera ray).
 template <class Acc>
 __device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams& p, int px, int py,
-                                            const PathRng& rng, const float4* rec, int nv, float3 Lo, float3 delta,
-                                            Acc& mc, float* s_g, float* s_c, float* g_tex, float* g_tex_c,
-                                            RayCounts& rc) {
+                                            const PathRng& cam_rng, const PathRng& rng, const float4* rec, int nv,
+                                            float3 Lo, float3 delta, Acc& mc, float* s_g, float* s_c, float* g_tex,
+                                            float* g_tex_c, RayCounts& rc) {
     if (nv == 0 || !isfinite(Lo.x) || !isfinite(Lo.y) || !isfinite(Lo.z)) return;
     float clampf = 1.f;             // firefly clamp factor (detached)
     {
@@ -296,7 +298,7 @@ __device__ __forceinline__ void replay_path(const DevScene& sc, const PathParams
         for (int k = 0; k < 64 && (c.x > kFirefly || c.y > kFirefly || c.z > kFirefly); ++k) { c *= 0.2f; clampf *= 0.2f; }
     }
     const float3 dp = delta * clampf;
-    RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
+    RayF ray = camera_ray(sc.cam, px, py, cam_rng.u(kDimCamera), cam_rng.u(kDimCamera + 1));
     float3 T = mk(1.f, 1.f, 1.f), collected = mk(0.f, 0.f, 0.f);
     float cont = 1.f;
     bool matte = false;
@@ -376,8 +378,10 @@ __device__ __forceinline__ void flush_block(const float* s_g, const float* s_c, 
     }
 }
 
-// Megakernel form: one thread per pixel runs pass 1 (forward with tracing, records in
-// thread-local memory) and pass 2 for each of its samples.
+// Megakernel form: one thread per pixel runs, for each of its camera samples, pass 1
+// (forward with tracing, records in thread-local memory) and pass 2 of each path. With
+// light samples a camera sample's n paths start at its camera ray's first hit (traced
+// once) and draw from sample indices s * L + j (integrate_camera_sample).
 __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p, const float4* __restrict__ dfilm,
                                                        int nmat, float* g_mat, float* g_mat_c, float* g_tex,
                                                        float* g_tex_c, unsigned long long* counters) {
@@ -386,28 +390,39 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
     __syncthreads();
     const int npix = sc.cam.w * sc.cam.h;
     const int pixel = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lmax = p.light_samples > 1 ? p.light_samples : 1;
     RayCounts rc;
     MatCache mc;
+    uint32_t paths = 0;
     if (pixel < npix) {
         const float4 df = dfilm[pixel];
         const float inv = 1.f / (float)p.spp;
         const float3 delta = mk(df.x * inv, df.y * inv, df.z * inv);
         const int px = pixel % sc.cam.w, py = pixel / sc.cam.w;
-        PathRng rng;
-        rng.key = seed_key(p.seed);
+        PathRng cam_rng;
+        cam_rng.key = seed_key(p.seed);
         const bool any = delta.x != 0.f || delta.y != 0.f || delta.z != 0.f;
         for (int s = 0; any && s < p.spp; ++s) {
-            rng.base = path_base((uint32_t)pixel, (uint32_t)(p.sample_offset + s));
-            // ---------------- pass 1: forward, recording hits and visibility
-            float4 rec[kAdjMaxDepth];
-            int nv = 0;
-            float3 Lo = mk(0.f, 0.f, 0.f);
-            {
-                RayF ray = camera_ray(sc.cam, px, py, rng.u(kDimCamera), rng.u(kDimCamera + 1));
-                const float3 cam_d = ray.d;
-                Hit h;
-                ++rc.closest;
-                if (bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
+            const int pass = p.sample_offset + s;
+            const int n = pass == 0 ? 1 : lmax;
+            cam_rng.base = path_base((uint32_t)pixel, (uint32_t)(pass * lmax));
+            RayF ray0 = camera_ray(sc.cam, px, py, cam_rng.u(kDimCamera), cam_rng.u(kDimCamera + 1));
+            const float3 cam_d = ray0.d;
+            Hit h0;
+            ++rc.closest;
+            if (!bvh_closest(sc.nodes, sc.tris, ray0.o, ray0.d, ray0.mint, ray0.maxt, &h0, rc.work)) continue;
+            const float3 dn = n > 1 ? delta * (1.f / (float)n) : delta;
+            for (int j = 0; j < n; ++j) {
+                PathRng rng = cam_rng;
+                rng.base = path_base((uint32_t)pixel, (uint32_t)(pass * lmax + j));
+                ++paths;
+                // ---------------- pass 1: forward, recording hits and visibility
+                float4 rec[kAdjMaxDepth];
+                int nv = 0;
+                float3 Lo = mk(0.f, 0.f, 0.f);
+                {
+                    RayF ray = ray0;
+                    Hit h = h0;
                     float3 T = mk(1.f, 1.f, 1.f);
                     float cont = 1.f;
                     bool matte = false;
@@ -444,14 +459,14 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         }
                     }
                 }
+                // ---------------- pass 2: re-shade the recorded vertices, accumulate gradients
+                replay_path(sc, p, px, py, cam_rng, rng, rec, nv, Lo, dn, mc, s_g, s_c, g_tex, g_tex_c, rc);
             }
-            // ---------------- pass 2: re-shade the recorded vertices, accumulate gradients
-            replay_path(sc, p, px, py, rng, rec, nv, Lo, delta, mc, s_g, s_c, g_tex, g_tex_c, rc);
         }
     }
     mc.flush(s_g, s_c);
     flush_block(s_g, s_c, nmat, g_mat, g_mat_c);
-    unsigned long long v[3] = {rc.closest, rc.shadow, pixel < npix ? (unsigned long long)p.spp : 0ull};
+    unsigned long long v[3] = {rc.closest, rc.shadow, paths};
 #pragma unroll
     for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -460,9 +475,11 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
         for (int k = 0; k < 3; ++k) atomicAdd(&counters[k], v[k]);
 }
 
-// Replay form (pass 2 only): one thread per item of a record pass (sample-major:
-// sl * npix + pixel, sample index p.sample_offset + s0 + sl). The wavefront engine's
-// record pass wrote the hit records rec[item][p.max_depth] and lo_raw[item].
+// Replay form (pass 2 only): one thread per item of a record pass (sub-sample-major:
+// q * npix + pixel with q = sl * L + j, L = max(1, light_samples), camera sample
+// p.sample_offset + s0 + sl, random-number sample index (p.sample_offset + s0) * L + q).
+// The wavefront engine's record pass wrote the hit records rec[item][p.max_depth] and
+// lo_raw[item]; the sub-samples j > 0 of the render's sample 0 were not traced.
 // 8 resident blocks of 128 threads (64 registers). (A grid-stride loop over a resident
 // grid was 30% slower: the block scheduler already balances 128-thread blocks.)
 __global__ void __launch_bounds__(kAdjBlock, 8) k_adjoint_replay(DevScene sc, PathParams p, int s0, uint32_t items,
@@ -478,16 +495,22 @@ __global__ void __launch_bounds__(kAdjBlock, 8) k_adjoint_replay(DevScene sc, Pa
     DirectAcc mc;
     const uint32_t item = blockIdx.x * blockDim.x + threadIdx.x;
     if (item < items) {
-        const uint32_t pixel = item % npix, sl = item / npix;
+        const uint32_t lsub = p.light_samples > 1 ? (uint32_t)p.light_samples : 1u;
+        const uint32_t pixel = item % npix, q = item / npix;
+        const uint32_t j = q % lsub, sample = (uint32_t)(p.sample_offset + s0) + q / lsub;
+        const uint32_t n = sample == 0 ? 1u : lsub;
         const float4 df = dfilm[pixel];
         const float inv = 1.f / (float)p.spp;
-        const float3 delta = mk(df.x * inv, df.y * inv, df.z * inv);
-        if (delta.x != 0.f || delta.y != 0.f || delta.z != 0.f) {
-            PathRng rng;
-            rng.key = seed_key(p.seed);
-            rng.base = path_base(pixel, (uint32_t)(p.sample_offset + s0) + sl);
+        float3 delta = mk(df.x * inv, df.y * inv, df.z * inv);
+        if (n > 1) delta = delta * (1.f / (float)n);
+        if (j < n && (delta.x != 0.f || delta.y != 0.f || delta.z != 0.f)) {
+            const uint32_t first = (uint32_t)(p.sample_offset + s0) * lsub;
+            PathRng rng, cam_rng;
+            rng.key = cam_rng.key = seed_key(p.seed);
+            rng.base = path_base(pixel, first + q);
+            cam_rng.base = path_base(pixel, first + q - j);
             const float4 lo = lo_raw[item];
-            replay_path(sc, p, (int)(pixel % (uint32_t)sc.cam.w), (int)(pixel / (uint32_t)sc.cam.w), rng,
+            replay_path(sc, p, (int)(pixel % (uint32_t)sc.cam.w), (int)(pixel / (uint32_t)sc.cam.w), cam_rng, rng,
                         rec + (size_t)item * p.max_depth, __float_as_int(lo.w), mk(lo.x, lo.y, lo.z), delta, mc, s_g,
                         s_c, g_tex, g_tex_c, rc);
         }
@@ -513,11 +536,13 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
     PathParams p;
     aur_status st = render_options(sc, o, &p);
     if (st != AUR_OK) return st;
-    if (o->max_depth > kAdjMaxDepth) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: max_depth above 16");
-    if (p.light_samples > 1) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: light_samples > 1");
     if (o->mode != AUR_RENDER_PLAIN && o->mode != AUR_RENDER_WAVEFRONT)
         return fail(AUR_ERR_INVALID_ARG, "aur_render_adjoint: unknown mode");
     const bool wavefront = o->mode == AUR_RENDER_WAVEFRONT;
+    // the megakernel keeps a path's hit records in registers / local memory; the wavefront
+    // form records them in device memory and takes any depth
+    if (!wavefront && o->max_depth > kAdjMaxDepth)
+        return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: max_depth above 16 needs mode AUR_RENDER_WAVEFRONT");
     if (sc->ntri >= (1u << 30)) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: 2^30 triangles or more");
     const int nmat = (int)sc->h_mats.size();
     if (nmat > kAdjMaxMat) return fail(AUR_ERR_UNSUPPORTED, "aur_render_adjoint: more than 64 materials");
@@ -551,13 +576,14 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
     if (wavefront) {
         // record passes (wavefront engine) + replay kernels over chunks of the samples, sized
         // so that the records stay within 2 GiB and item indices within 2^31
+        const size_t lsub = (size_t)p.light_samples;   // items per pixel and camera sample
         const size_t per_item = sizeof(float4) * ((size_t)p.max_depth + 1);
         const size_t budget = (size_t)2 << 30;
-        int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)p.spp, budget / (per_item * npix)));
-        while (chunk > 1 && (size_t)chunk * npix * (p.max_depth + 1) >= (1ull << 31)) chunk /= 2;
-        if ((size_t)chunk * npix * (p.max_depth + 1) >= (1ull << 31)) e = cudaErrorInvalidValue;
-        if (e == cudaSuccess) e = ctx_scratch(sc->ctx, per_item * npix * chunk, (void**)&rec);
-        float4* lo_raw = rec ? rec + (size_t)npix * chunk * p.max_depth : nullptr;
+        int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)p.spp, budget / (per_item * npix * lsub)));
+        while (chunk > 1 && (size_t)chunk * npix * lsub * (p.max_depth + 1) >= (1ull << 31)) chunk /= 2;
+        if ((size_t)chunk * npix * lsub * (p.max_depth + 1) >= (1ull << 31)) e = cudaErrorInvalidValue;
+        if (e == cudaSuccess) e = ctx_scratch(sc->ctx, per_item * npix * lsub * chunk, (void**)&rec);
+        float4* lo_raw = rec ? rec + (size_t)npix * lsub * chunk * p.max_depth : nullptr;
         for (int s0 = 0; s0 < p.spp && e == cudaSuccess; s0 += chunk) {
             const int n = std::min(chunk, p.spp - s0);
             aur_status rs = wf_record_pass(sc, p, s0, n, rec, lo_raw, &launches, rays);
@@ -569,7 +595,7 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
                 cudaEventDestroy(er1);
                 return rs;
             }
-            const uint32_t items = (uint32_t)(npix * (size_t)n);
+            const uint32_t items = (uint32_t)(npix * lsub * (size_t)n);
             cudaEventRecord(er0, s);
             k_adjoint_replay<<<(items + kAdjBlock - 1) / kAdjBlock, kAdjBlock, 0, s>>>(
                 sc->dev(), p, s0, items, rec, lo_raw, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
@@ -597,7 +623,11 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
     cudaEventRecord(e1, s);
     if (e == cudaSuccess) e = gm.finish();
     if (e == cudaSuccess && ntex) e = gt.finish();
-    unsigned long long cnt[3] = {rays[0], rays[1], (unsigned long long)npix * p.spp};
+    // paths traced: the render's sample 0 traces one path, every other camera sample L
+    const unsigned long long lpaths = (unsigned long long)p.light_samples;
+    unsigned long long cnt[3] = {rays[0], rays[1],
+                                 (unsigned long long)npix * ((unsigned long long)p.spp * lpaths -
+                                                             (p.sample_offset == 0 ? lpaths - 1 : 0))};
     if (e == cudaSuccess && !wavefront)
         e = cudaMemcpyAsync(cnt, sc->ctx->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
@@ -614,7 +644,7 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
         stats->closest_rays = cnt[0];
         stats->shadow_rays = cnt[1];
         stats->paths = cnt[2];
-        stats->camera_rays = cnt[2];
+        stats->camera_rays = (unsigned long long)npix * p.spp;
         stats->launches = launches;
         stats->kernel_ms = ms;
         if (wavefront) {   // stage_ms[0]: record passes (and the rest), stage_ms[1]: replay kernels

@@ -54,7 +54,13 @@ struct WfScene {
     PathParams p;          // spp = samples of this pass, sample_offset = first sample index of this pass
     uint64_t key;
     uint32_t npix, item_base, items, rec_depth;
-    float4* samples;       // [spp_pass][npix]
+    // Light samples: every camera sample of the pass has lsub sub-samples q = sl * lsub + j
+    // (lsub = light_samples, 1 without them); sub-sample j of sample s traces the path j of
+    // Integrator::integrateCameraSample(sample, numSamples) and draws from random-number sample
+    // index s * lsub + j = rng_offset + q, its camera ray from s * lsub. The render's sample 0
+    // has one path only (renderer.cpp:231-258): its sub-samples j > 0 are skipped.
+    uint32_t lsub, rng_offset;
+    float4* samples;       // [spp_pass * lsub][npix]
     // record mode (path-replay adjoint): per item (sample-major, sl * npix + pixel)
     float4* rec;           // [items][rec_depth] hit records (t, u, v, prim | visibility << 30)
     float4* lo_raw;        // [items] unclamped path radiance, w = number of recorded vertices
@@ -114,6 +120,16 @@ __device__ __forceinline__ void block_reserve(BlockScan& sh, const bool (&p)[3],
     __syncthreads();   // sh is reused by the next call
 }
 
+// random-number sample index of sub-sample q, and that of its camera ray
+__device__ __forceinline__ uint32_t rng_index(const WfScene& S, uint32_t q) { return S.rng_offset + q; }
+__device__ __forceinline__ uint32_t cam_index(const WfScene& S, uint32_t q) {
+    return S.lsub > 1 ? S.rng_offset + q - q % S.lsub : S.rng_offset + q;
+}
+// sub-samples j > 0 of the render's sample 0 trace nothing (one path in the first pass)
+__device__ __forceinline__ bool skipped_sub(const WfScene& S, uint32_t q) {
+    return S.lsub > 1 && q % S.lsub != 0 && (uint32_t)S.p.sample_offset + q / S.lsub == 0;
+}
+
 __device__ __forceinline__ int scene_of(const WfPool& w, uint32_t item) {
     int lo = 0, hi = w.nscenes - 1;
     while (lo < hi) {
@@ -162,7 +178,10 @@ __global__ void k_regen(WfPool w, int in_q) {
                 S.lo_raw[(size_t)id.z * S.npix + id.y] = make_float4(lo.x, lo.y, lo.z, __int_as_float(f_vtx(id.w)));
             } else {
                 const float3 L = (id.w & kNoClamp) ? mk(lo.x, lo.y, lo.z) : firefly_clamp(mk(lo.x, lo.y, lo.z));
-                S.samples[(size_t)id.z * S.npix + id.y] = make_float4(L.x, L.y, L.z, lo.w);
+                // with light samples, alpha 2 marks the environment seen by the camera ray: the
+                // sample is that radiance, not the mean of its sub-samples (integrator.cpp:287-298)
+                const float a = (S.lsub > 1 && (id.w & kNoClamp)) ? 2.f : lo.w;
+                S.samples[(size_t)id.z * S.npix + id.y] = make_float4(L.x, L.y, L.z, a);
             }
             st = PS_EMPTY;
         }
@@ -175,22 +194,28 @@ __global__ void k_regen(WfPool w, int in_q) {
             block_reserve(s_scan, pw, cw, pos);
             if (want) item = pos[0];
         }
-        const bool start = want && item < total;
+        bool start = want && item < total;
+        int s = 0;
+        uint32_t pixel = 0, q = 0;
         if (start) {
-            const int s = scene_of(w, item);
+            s = scene_of(w, item);
+            const uint32_t local = item - w.scenes[s].item_base;
+            pixel = local % w.scenes[s].npix;
+            q = local / w.scenes[s].npix;
+            start = !skipped_sub(w.scenes[s], q);
+        }
+        if (start) {
             const WfScene& S = w.scenes[s];
-            const uint32_t local = item - S.item_base;
-            const uint32_t pixel = local % S.npix, sl = local / S.npix;
             PathRng rng;
             rng.key = S.key;
-            rng.base = path_base(pixel, (uint32_t)S.p.sample_offset + sl);
+            rng.base = path_base(pixel, cam_index(S, q));
             const RayF r = camera_ray(S.sc.cam, (int)(pixel % (uint32_t)S.sc.cam.w), (int)(pixel / (uint32_t)S.sc.cam.w),
                                       rng.u(kDimCamera), rng.u(kDimCamera + 1));
             w.ray_o[i] = make_float4(r.o.x, r.o.y, r.o.z, r.mint);
             w.ray_d[i] = make_float4(r.d.x, r.d.y, r.d.z, r.maxt);
             w.tp[i] = make_float4(1.f, 1.f, 1.f, 1.f);
             w.lo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            w.id[i] = make_uint4((uint32_t)s, pixel, sl, pack_flags(0, 0, RAY_CAMERA, false));
+            w.id[i] = make_uint4((uint32_t)s, pixel, q, pack_flags(0, 0, RAY_CAMERA, false));
             st = PS_ACTIVE;
         }
         {
@@ -346,7 +371,7 @@ __device__ __noinline__ float4 shade_env_miss(uint4* ids, const float4* tp, cons
                                               int vtx, float4 lo) {
     PathRng rng;
     rng.key = S->key;
-    rng.base = path_base(id.y, (uint32_t)S->p.sample_offset + id.z);
+    rng.base = path_base(id.y, cam_index(*S, id.z));
     const RayF cr = camera_ray(S->sc.cam, (int)(id.y % (uint32_t)S->sc.cam.w), (int)(id.y / (uint32_t)S->sc.cam.w),
                                rng.u(kDimCamera), rng.u(kDimCamera + 1));
     const float3 e = env_radiance_of(S->sc.sh.lights, S->sc.sh.nlights, S->sc.sh.texs, S->sc.sh.texels, cr.d);
@@ -405,7 +430,7 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 int bounces = f_bounces(flags);
                 PathRng rng;
                 rng.key = S.key;
-                rng.base = path_base(id.y, (uint32_t)S.p.sample_offset + id.z);
+                rng.base = path_base(id.y, rng_index(S, id.z));
                 const float4 ro = w.ray_o[slot], rd = w.ray_d[slot];
                 float4 tpv = w.tp[slot];
                 float3 T = mk(tpv.x, tpv.y, tpv.z);
@@ -581,10 +606,35 @@ __global__ void k_resolve(const WfScene* scenes, int s, float4* acc_s, float4* a
     k.s = mk(a.x, a.y, a.z);
     k.c = mk(c.x, c.y, c.z);
     float alpha = a.w;
-    for (int j = 0; j < S.p.spp; ++j) {
-        const float4 v = S.samples[(size_t)j * S.npix + pixel];
-        k.add(mk(v.x, v.y, v.z));
-        alpha += v.w;
+    if (S.lsub <= 1) {
+        for (int j = 0; j < S.p.spp; ++j) {
+            const float4 v = S.samples[(size_t)j * S.npix + pixel];
+            k.add(mk(v.x, v.y, v.z));
+            alpha += v.w;
+        }
+    } else {
+        // a camera sample with light samples is the mean of its n sub-samples, added in their
+        // order as Lo / n (integrate_camera_sample); n = 1 for the render's sample 0
+        for (int sl = 0; sl < S.p.spp; ++sl) {
+            const float4* sub = S.samples + (size_t)sl * S.lsub * S.npix + pixel;
+            const float4 v0 = sub[0];
+            if (v0.w == 2.f) {               // the camera ray saw the environment
+                k.add(mk(v0.x, v0.y, v0.z));
+                alpha += 1.f;
+                continue;
+            }
+            const int n = S.p.sample_offset + sl == 0 ? 1 : (int)S.lsub;
+            float3 sum = mk(v0.x, v0.y, v0.z);
+            if (n > 1) {
+                sum = cdiv(sum, (float)n);
+                for (int j = 1; j < n; ++j) {
+                    const float4 v = sub[(size_t)j * S.npix];
+                    sum += cdiv(mk(v.x, v.y, v.z), (float)n);
+                }
+            }
+            k.add(sum);
+            alpha += v0.w;
+        }
     }
     acc_s[pixel] = make_float4(k.s.x, k.s.y, k.s.z, alpha);
     acc_c[pixel] = make_float4(k.c.x, k.c.y, k.c.z, 0.f);
@@ -805,6 +855,13 @@ struct BatchItem {
     uint32_t npix;
     float4* acc_s;
     float4* acc_c;
+    uint32_t lsub() const { return p.light_samples > 1 ? (uint32_t)p.light_samples : 1u; }
+    // work items (one per traced or skipped sub-sample) of one camera sample of every pixel
+    uint64_t items_per_sample() const { return (uint64_t)npix * lsub(); }
+    // paths traced for spp samples from sample_offset (the render's sample 0 traces one)
+    uint64_t paths(int spp, int offset) const {
+        return (uint64_t)npix * ((uint64_t)spp * lsub() - (offset == 0 && spp > 0 ? lsub() - 1 : 0));
+    }
 };
 
 // Fills the scene table of one pass: samples [s0, s0 + chunk) of every scene.
@@ -824,11 +881,13 @@ static uint32_t fill_table(std::vector<BatchItem>& items, int s0, int chunk, flo
         t.p.sample_offset = items[i].p.sample_offset + s0;
         t.key = seed_key(items[i].p.seed);
         t.npix = items[i].npix;
+        t.lsub = items[i].lsub();
+        t.rng_offset = (uint32_t)t.p.sample_offset * t.lsub;
         t.item_base = base;
-        t.items = t.npix * (uint32_t)pass_spp;
-        t.samples = samples + off;
+        t.items = (uint32_t)(items[i].items_per_sample() * (uint32_t)pass_spp);
+        t.samples = samples ? samples + off : nullptr;
         base += t.items;
-        off += (size_t)t.npix * chunk;
+        off += (size_t)items[i].items_per_sample() * chunk;
     }
     return base;
 }
@@ -843,12 +902,19 @@ static aur_status autotune(aur_ctx* ctx, std::vector<BatchItem>& items, WfConfig
     cudaStream_t s = ctx->work_stream;
     size_t per_sample = 0;
     uint64_t total = 0;
-    for (auto& it : items) { per_sample += (size_t)it.npix * sizeof(float4); total += (uint64_t)it.npix * it.p.spp; }
+    for (auto& it : items) {
+        per_sample += (size_t)it.items_per_sample() * sizeof(float4);
+        total += it.items_per_sample() * it.p.spp;
+    }
     const uint32_t limit = (uint32_t)std::min<uint64_t>(total, 1ull << 25);
     int chunk = 1;   // samples buffer large enough for the probe's first `limit` items
     {
-        uint32_t covered = 0;
-        while (covered < limit) { covered = 0; for (auto& it : items) covered += it.npix * std::min(chunk, it.p.spp); ++chunk; }
+        uint64_t covered = 0;
+        while (covered < limit) {
+            covered = 0;
+            for (auto& it : items) covered += it.items_per_sample() * std::min(chunk, it.p.spp);
+            ++chunk;
+        }
     }
     float4* samples = nullptr;
     cudaError_t e = cudaMallocAsync(&samples, per_sample * chunk, s);
@@ -960,11 +1026,16 @@ static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, c
     const size_t budget = (size_t)3 << 30;
     size_t per_sample = 0;
     int max_spp = 0;
-    for (auto& it : items) { per_sample += (size_t)it.npix * sizeof(float4); max_spp = std::max(max_spp, it.p.spp); }
+    for (auto& it : items) {
+        per_sample += (size_t)it.items_per_sample() * sizeof(float4);
+        max_spp = std::max(max_spp, it.p.spp);
+    }
     const int chunk = (int)std::max<size_t>(1, std::min<size_t>((size_t)max_spp, budget / std::max<size_t>(per_sample, 1)));
     e = run.ensure_samples(per_sample * chunk);
     float4* samples = run.samples;
-    if (e == cudaSuccess) e = run.ensure_acc(2 * per_sample);   // two float4 per pixel
+    size_t per_pixel_set = 0;
+    for (auto& it : items) per_pixel_set += (size_t)it.npix * sizeof(float4);
+    if (e == cudaSuccess) e = run.ensure_acc(2 * per_pixel_set);   // two float4 per pixel
     {
         size_t off = 0;
         for (auto& it : items) {
@@ -1022,10 +1093,10 @@ static aur_status wavefront_batch(aur_ctx* ctx, std::vector<BatchItem>& items, c
     if (e != cudaSuccess) return cuda_fail(e, "wavefront");
     *kernel_ms = ms;
     if (stats) {
-        uint64_t paths = 0;
-        for (auto& it : items) paths += (uint64_t)it.npix * it.p.spp;
+        uint64_t paths = 0, cams = 0;
+        for (auto& it : items) { paths += it.paths(it.p.spp, it.p.sample_offset); cams += (uint64_t)it.npix * it.p.spp; }
         stats->paths = paths;
-        stats->camera_rays = paths;
+        stats->camera_rays = cams;   // camera samples; with light samples every path retraces its camera ray
         stats->closest_rays = rays[0];
         stats->shadow_rays = rays[1];
         stats->launches = launches;
@@ -1110,7 +1181,8 @@ aur_status render_wavefront(aur_scene* sc, const aur_render_opts* o, float* film
     DeviceGuard g(sc->ctx->device);
     cudaStream_t s = sc->ctx->stream;
     const uint32_t npix = (uint32_t)sc->cam.w * sc->cam.h;
-    if ((uint64_t)npix * o->spp >= (1ull << 31)) return fail(AUR_ERR_INVALID_ARG, "aur_render: more than 2^31 paths");
+    if ((uint64_t)npix * o->spp * (uint64_t)p.light_samples >= (1ull << 31))
+        return fail(AUR_ERR_INVALID_ARG, "aur_render: more than 2^31 paths");
     DevOut fo;
     cudaError_t e = fo.init(film, sizeof(float4) * npix, 16, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);   // film staging allocated on the caller's stream
@@ -1171,7 +1243,7 @@ extern "C" aur_status aur_render_batch(aur_scene* const* scenes, const aur_rende
         PathParams p;
         if ((st = render_options(scenes[i], &opts[i], &p)) != AUR_OK) return st;
         const uint32_t npix = (uint32_t)scenes[i]->cam.w * scenes[i]->cam.h;
-        total += (uint64_t)npix * p.spp;
+        total += (uint64_t)npix * p.spp * (uint64_t)p.light_samples;
         items[i] = {scenes[i], p, npix, nullptr, nullptr};
     }
     if (total >= (1ull << 31)) return fail(AUR_ERR_INVALID_ARG, "aur_render_batch: more than 2^31 paths");

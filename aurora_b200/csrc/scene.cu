@@ -378,8 +378,6 @@ aur_status render_options(const aur_scene* sc, const aur_render_opts* o, PathPar
     const long long lmax = o->light_samples > 1 ? o->light_samples : 1;
     if (o->sample_offset < 0 || ((long long)o->sample_offset + o->spp) * lmax > (1 << 20))
         return fail(AUR_ERR_INVALID_ARG, "render: sample indices (times light_samples) must stay below 2^20");
-    if (lmax > 1 && o->mode != AUR_RENDER_PLAIN)
-        return fail(AUR_ERR_UNSUPPORTED, "render: light_samples > 1 is rendered by the plain renderer (mode 0)");
     if (lmax > 1 && o->count_work) return fail(AUR_ERR_UNSUPPORTED, "render: count_work with light_samples > 1");
     p->light_samples = (int)lmax;
     p->max_depth = o->max_depth;

@@ -1087,8 +1087,6 @@ struct Loader {
         out.opts.wf_sort = -1;
         if (out.light_samples < 1) throw_load(AUR_ERR_PARSE, "options: lightsamples must be >= 1");
         out.opts.light_samples = out.light_samples;
-        // several paths per camera sample are rendered by the plain renderer
-        if (out.light_samples > 1) out.opts.mode = AUR_RENDER_PLAIN;
         out.output = need_str(*opt, "filename", "options");
         // camera (parseCamera, jsonParser.cpp:476-502)
         const JValue* cam = root.get("renderCam");

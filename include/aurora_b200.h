@@ -252,8 +252,10 @@ typedef struct aur_render_opts {
                                integrator.cpp:152-300; renderer.cpp:231-258): 0 or 1 = one path per
                                camera sample; L > 1 = the render's first pass (sample index 0)
                                traces one path, every later pass L paths from the camera ray's
-                               first hit, each firefly-filtered, averaged. Plain renderer only;
-                               (sample_offset + spp) * L must stay below 2^20. */
+                               first hit, each firefly-filtered, averaged. Both renderers and
+                               the adjoint; the wavefront renderer retraces the camera ray for
+                               each path (closest_rays counts it). (sample_offset + spp) * L must
+                               stay below 2^20. */
 } aur_render_opts;
 
 /* ------------------------------------------------------------ scene files
@@ -349,7 +351,9 @@ AUR_API aur_status aur_render_batch(aur_scene* const* scenes, const aur_render_o
 
 /* Path-replay adjoint: given dLoss/dFilm (width*height*4 floats, alpha
  * ignored) accumulates gradients into grad_mat (nmat x 4) and grad_tex
- * (ntexel_floats). Both are overwritten. */
+ * (ntexel_floats). Both are overwritten. Mode AUR_RENDER_WAVEFRONT (record pass on
+ * the wavefront engine + replay kernel) takes any max_depth; AUR_RENDER_PLAIN (one
+ * megakernel) at most 16. light_samples as for aur_render. */
 AUR_API aur_status aur_render_adjoint(aur_scene* scene, const aur_render_opts* opts, const float* dloss_dfilm,
                               float* grad_mat, float* grad_tex, aur_render_stats* stats);
 

@@ -1226,10 +1226,12 @@ static void envMiss(const Scene& sc, const Vector& camDir, const Color& T, const
     }
 }
 
-static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& rng, int maxDepth, int minDepth,
-                                const double delta[3], double* grad) {
+// camRng draws the camera ray (with light samples the paths of a camera sample share it),
+// rng the path's decisions; delta = dLoss/dpixel / spp (/ n for one of n light-sample paths).
+static void adjointCameraSample(const Scene& sc, int x, int y, const Rng& camRng, const Rng& rng, int maxDepth,
+                                int minDepth, const double delta[3], double* grad) {
     Counts cnt;
-    Ray ray = convertSample(sc, x, y, rng(0), rng(1));
+    Ray ray = convertSample(sc, x, y, camRng(0), camRng(1));
     const Vector camDir = ray.direction;
     int prim; float t, u, v;
     if (!sceneIntersect(sc, ray, &prim, &t, &u, &v)) return;   // the environment alone: no parameter
@@ -1619,8 +1621,10 @@ int oracle_render(void* h, int spp, int sample_offset, int max_depth, int min_de
 // dLoss/dparams of <dfilm, image> restricted to pixels [x0, x0+w) x [y0, y0+h), with
 // dfilm the full W*H*4 image gradient (alpha ignored) and the image the spp-sample mean.
 // grad: 4*nmat + ntexel_floats doubles (overwritten).
+// light_samples L > 1: camera sample s (s > 0) has L paths from its camera ray's first hit,
+// drawing from sample indices s L + j and weighted 1 / L (integrateCameraSample(sample, L)).
 int oracle_adjoint(void* h, int spp, int sample_offset, int max_depth, int min_depth, uint32_t seed, int threads,
-                   int x0, int y0, int w, int hgt, const float* dfilm, double* grad) {
+                   int x0, int y0, int w, int hgt, const float* dfilm, double* grad, int light_samples) {
     const Scene& sc = *(Scene*)h;
     const size_t np = 4 * sc.mats.size() + sc.texels.size();
     if (threads > 0) omp_set_num_threads(threads);
@@ -1636,10 +1640,18 @@ int oracle_adjoint(void* h, int spp, int sample_offset, int max_depth, int min_d
             const double delta[3] = {(double)dfilm[4 * (size_t)pixel] / spp, (double)dfilm[4 * (size_t)pixel + 1] / spp,
                                      (double)dfilm[4 * (size_t)pixel + 2] / spp};
             if (delta[0] == 0 && delta[1] == 0 && delta[2] == 0) continue;
+            const int lmax = light_samples > 1 ? light_samples : 1;
             for (int s = 0; s < spp; ++s) {
-                Rng rng; rng.key = key;
-                rng.base = ((uint64_t)pixel << 32) | ((uint64_t)(sample_offset + s) << 12);
-                adjointCameraSample(sc, x, y, rng, max_depth, min_depth, delta, local.data());
+                const int pass = sample_offset + s;
+                const int n = pass == 0 ? 1 : lmax;
+                const double dn[3] = {delta[0] / n, delta[1] / n, delta[2] / n};
+                Rng cam; cam.key = key;
+                cam.base = ((uint64_t)pixel << 32) | ((uint64_t)(pass * lmax) << 12);
+                for (int j = 0; j < n; ++j) {
+                    Rng rng = cam;
+                    rng.base = ((uint64_t)pixel << 32) | ((uint64_t)(pass * lmax + j) << 12);
+                    adjointCameraSample(sc, x, y, cam, rng, max_depth, min_depth, dn, local.data());
+                }
             }
         }
 #pragma omp critical

@@ -41,7 +41,7 @@ def lib() -> C.CDLL:
         L.oracle_render.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp, vp, i32]
         L.oracle_kelemen_table.argtypes = [C.c_float, i32, u32, vp, i32]
         L.oracle_shading_probe.argtypes = [vp, i32, vp, u32, vp, vp]
-        L.oracle_adjoint.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp]
+        L.oracle_adjoint.argtypes = [vp, i32, i32, i32, i32, u32, i32, i32, i32, i32, i32, vp, vp, i32]
         _lib = L
     return _lib
 
@@ -129,7 +129,7 @@ class OracleScene:
                             int(light_samples))
         return mean, m2, counts
 
-    def adjoint(self, spp, max_depth, min_depth, seed, dfilm, crop=None, sample_offset=0, threads=0):
+    def adjoint(self, spp, max_depth, min_depth, seed, dfilm, crop=None, sample_offset=0, threads=0, light_samples=1):
         """FP64 gradient of <dfilm, image> w.r.t. (per material: diffuse rgb, roughness) and the
         texels, over the crop's pixels. Returns (grad_mat [nmat, 4], grad_tex [ntexel floats])."""
         W, H = self.data.width, self.data.height
@@ -139,7 +139,7 @@ class OracleScene:
         ntex = int(self.data.texels().size)
         grad = np.zeros(4 * nmat + ntex, np.float64)
         lib().oracle_adjoint(self.h, spp, sample_offset, max_depth, min_depth, seed, threads, x0, y0, w, h,
-                             dfilm.ctypes.data, grad.ctypes.data)
+                             dfilm.ctypes.data, grad.ctypes.data, int(light_samples))
         return grad[:4 * nmat].reshape(nmat, 4), grad[4 * nmat:]
 
     def probe(self, kind, records):

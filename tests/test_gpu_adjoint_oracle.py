@@ -23,7 +23,7 @@ def _compare(gpu, cpu, what):
     assert np.all(err <= bound), what
 
 
-def _run(ctx, kelemen_tables, oracle_lib, data, crop, spp, seed, wseed, mode):
+def _run(ctx, kelemen_tables, oracle_lib, data, crop, spp, seed, wseed, mode, light_samples=1):
     import aurora_b200 as ab
     H, W = data.height, data.width
     w = np.zeros((H, W, 4), np.float32)
@@ -31,10 +31,10 @@ def _run(ctx, kelemen_tables, oracle_lib, data, crop, spp, seed, wseed, mode):
     w[y0:y0 + ch, x0:x0 + cw, :3] = np.random.default_rng(wseed).normal(size=(ch, cw, 3))
     depth, mind = data.render["max_depth"], data.render["min_depth"]
     scene = ab.Scene(ctx, data)
-    gm, gt, _ = scene.adjoint(ab.render_opts(spp, depth, mind, seed, mode=mode), w)
+    gm, gt, _ = scene.adjoint(ab.render_opts(spp, depth, mind, seed, mode=mode, light_samples=light_samples), w)
     scene.close()
     osc = oracle_lib.OracleScene(data, kelemen_tables, use_bvh=True)
-    cm, ct = osc.adjoint(spp, depth, mind, seed, w, crop=crop)
+    cm, ct = osc.adjoint(spp, depth, mind, seed, w, crop=crop, light_samples=light_samples)
     return gm, gt, cm, ct
 
 
@@ -121,3 +121,34 @@ def test_adjoint_matches_fp64_oracle_texture_shaders(ctx, kelemen_tables, oracle
     assert np.count_nonzero(ct) > 100
     _compare(gm, cm, "materials (diffuse rgb, roughness)")
     _compare(gt, ct, "texels")
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_adjoint_matches_fp64_oracle_light_samples(ctx, kelemen_tables, oracle_lib, mode):
+    """light_samples 3 on the differentiable workload: every camera sample after the first has
+    three paths from its camera ray's first hit, each replayed with weight 1/3."""
+    from aurora_b200 import scenes
+    data = scenes.texture_scene()
+    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (112, 180, 32, 32), 16, 2, 28, mode,
+                          light_samples=3)
+    assert np.count_nonzero(ct) > 100
+    _compare(gm, cm, "materials (light samples 3)")
+    _compare(gt, ct, "texels (light samples 3)")
+
+
+def test_adjoint_deeper_than_16_wavefront(ctx, kelemen_tables, oracle_lib):
+    """max_depth 20 (glass boxes, roulette from the second bounce): the wavefront adjoint records
+    hits in device memory and takes any depth; the megakernel refuses more than 16."""
+    import aurora_b200 as ab
+    from aurora_b200 import _abi, scenes
+    glass = dict(type_=_abi.MAT_GLASS, specular=(1.0, 1.0, 1.0), diffuse=(0.95, 0.9, 0.85), reflectance=0.04,
+                 ior=1.5)
+    data = scenes.box_scene(128, 128, spp=32, max_depth=20, box_mat=glass, lift=0.01)
+    data.render["min_depth"] = 1
+    gm, gt, cm, ct = _run(ctx, kelemen_tables, oracle_lib, data, (40, 72, 32, 32), 32, 1, 29, 1)
+    _compare(gm, cm, "materials (depth 20)")
+    scene = ab.Scene(ctx, data)
+    with pytest.raises(ab.AuroraError) as e:
+        scene.adjoint(ab.render_opts(4, 20, 1, 1, mode=0), np.zeros((128, 128, 4), np.float32))
+    assert e.value.status == _abi.ERR_UNSUPPORTED
+    scene.close()

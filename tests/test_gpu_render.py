@@ -162,22 +162,24 @@ def test_progressive_passes(ctx, mode):
     scene.close()
 
 
-def test_light_samples(ctx, oracle_lib, kelemen_tables):
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_light_samples(ctx, oracle_lib, kelemen_tables, mode):
     """light_samples 4: passes after the first trace four paths from the camera ray's first
-    hit, on the device as in the oracle; the wavefront renderer and the adjoint refuse it."""
+    hit, each firefly-filtered and added as Lo / 4, on the device as in the oracle; the plain
+    and the wavefront renderer give the same film. Also from a sample offset (no first pass)."""
     import aurora_b200 as ab
-    from aurora_b200 import _abi, scenes
-    data = scenes.sphere_scene(48, 48)
+    from aurora_b200 import scenes
+    data = scenes.sphere_scene(48, 48, env=dict(color=(0.3, 0.35, 0.4)))
     scene = ab.Scene(ctx, data)
-    res = scene.render(ab.render_opts(8, 6, 6, 2, light_samples=4))
-    mean, m2, counts = oracle_lib.OracleScene(data, kelemen_tables).render(8, 6, 6, 2, light_samples=4)
-    compare(res.film, mean, m2, 8)          # 8 passes: the alpha means are exact in float
-    assert res.stats["paths"] == 48 * 48 * (1 + 7 * 4) == int(counts[2])
-    for call in (lambda: scene.render(ab.render_opts(6, 6, 6, 2, mode=_abi.RENDER_WAVEFRONT, light_samples=4)),
-                 lambda: scene.adjoint(ab.render_opts(6, 6, 6, 2, light_samples=4), np.zeros((48, 48, 4), np.float32))):
-        with pytest.raises(ab.AuroraError) as e:
-            call()
-        assert e.value.status == _abi.ERR_UNSUPPORTED
+    osc = oracle_lib.OracleScene(data, kelemen_tables)
+    for offset in (0, 5):
+        res = scene.render(ab.render_opts(8, 6, 6, 2, mode=mode, light_samples=4, sample_offset=offset))
+        mean, m2, counts = osc.render(8, 6, 6, 2, light_samples=4, sample_offset=offset)
+        compare(res.film, mean, m2, 8)          # 8 passes: the alpha means are exact in float
+        assert res.stats["paths"] == 48 * 48 * (8 * 4 - (3 if offset == 0 else 0)) == int(counts[2])
+        if mode == 1:
+            plain = scene.render(ab.render_opts(8, 6, 6, 2, light_samples=4, sample_offset=offset)).film
+            np.testing.assert_allclose(res.film, plain, rtol=1e-6, atol=1e-7)
     scene.close()
 
 

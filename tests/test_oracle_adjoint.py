@@ -12,9 +12,10 @@ import numpy as np
 import pytest
 
 
-def _loss(oracle_lib, data, tables, w, spp, crop, seed):
+def _loss(oracle_lib, data, tables, w, spp, crop, seed, light_samples=1):
     osc = oracle_lib.OracleScene(data, tables, use_bvh=True)
-    mean, _, _ = osc.render(spp, data.render["max_depth"], data.render["min_depth"], seed, crop=crop, want_m2=False)
+    mean, _, _ = osc.render(spp, data.render["max_depth"], data.render["min_depth"], seed, crop=crop, want_m2=False,
+                            light_samples=light_samples)
     x0, y0, cw, ch = crop
     return float(np.sum(mean[..., :3] * w[y0:y0 + ch, x0:x0 + cw, :3]))
 
@@ -147,3 +148,20 @@ def test_oracle_adjoint_escape_after_last_vertex_matches_fd(oracle_lib):
         fd = (_loss(oracle_lib, _perturbed_material(data, 0, c, h), tables, w, spp, crop, seed) -
               _loss(oracle_lib, _perturbed_material(data, 0, c, -h), tables, w, spp, crop, seed)) / (2 * h)
         assert abs(gm[0, c] - fd) <= 0.01 * abs(fd) + 1e-6, (c, gm[0, c], fd)
+
+
+def test_oracle_adjoint_light_samples_matches_fd(oracle_lib):
+    """light_samples 3 (integrateCameraSample(sample, 3) after the first pass): the wall albedo
+    gradients of the oracle's adjoint against central differences of its renderer."""
+    from aurora_b200 import scenes
+    data = scenes.box_scene(48, 48, spp=4)
+    tables = np.zeros((21, 64, 32), np.float32)
+    w = np.random.default_rng(12).normal(size=(48, 48, 4)).astype(np.float32)
+    w[..., 3] = 0.0
+    crop, spp, seed = (8, 8, 32, 32), 4, 1
+    gm, _ = oracle_lib.OracleScene(data, tables).adjoint(spp, 5, 5, seed, w, crop=crop, light_samples=3)
+    h = 1e-2
+    for m, c in [(0, 0), (1, 0), (2, 1)]:
+        fd = (_loss(oracle_lib, _perturbed_material(data, m, c, h), tables, w, spp, crop, seed, 3) -
+              _loss(oracle_lib, _perturbed_material(data, m, c, -h), tables, w, spp, crop, seed, 3)) / (2 * h)
+        assert abs(gm[m, c] - fd) <= 0.01 * abs(fd) + 1e-6, (m, c, gm[m, c], fd)

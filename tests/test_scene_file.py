@@ -326,8 +326,8 @@ def test_json_syntax_error_names_the_line(tmp_path):
 
 
 def test_light_samples_option(tmp_path):
-    """The file's lightsamples reach the render options; several paths per camera sample
-    select the plain renderer."""
+    """The file's lightsamples reach the render options; the (wavefront) renderer the file
+    selects takes any number of paths per camera sample."""
     v, f = scenes.quad((-1, -1, 0), (1, -1, 0), (1, 1, 0), (-1, 1, 0))
     write_obj(str(tmp_path / "q.obj"), v, f, normals=np.tile([0, 0, 1.0], (4, 1)))
     p = write_single(str(tmp_path), "q.obj", 0)
@@ -335,7 +335,7 @@ def test_light_samples_option(tmp_path):
     s["options"]["lightsamples"] = 8
     json.dump(s, open(p, "w"))
     _, opts, info = scenes.load_scene_file(p)
-    assert opts.light_samples == 8 and opts.mode == _abi.RENDER_PLAIN and info["light_samples"] == 8
+    assert opts.light_samples == 8 and opts.mode == _abi.RENDER_WAVEFRONT and info["light_samples"] == 8
     s["options"]["lightsamples"] = 1
     json.dump(s, open(p, "w"))
     _, opts, _ = scenes.load_scene_file(p)
