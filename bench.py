@@ -234,6 +234,33 @@ def adjoint_ratio(ab, _abi, torch, ctx, stream, steps=2, warmup=1):
                     "wavefront forward (the autograd pair); ratio_plain: megakernel adjoint over the plain forward"}
 
 
+def batch_timing(ab, _abi, torch, ctx, stream, steps=3):
+    """The 64-scene batched workload: box scenes (seed 6+i) of resolution 128^2..512^2, 4/16/64
+    spp and depth 3/5/8 in one wavefront launch (autotuned once, untimed), films resident on
+    the device. Device time per launch (CUDA events, mean of `steps`) and path samples/s."""
+    from aurora_b200 import scenes
+    datas = scenes.batch_scenes(64)
+    objs = [ab.Scene(ctx, d) for d in datas]
+    opts = [ab.render_opts(d.render["spp"], d.render["max_depth"], d.render["min_depth"], d.render["seed"],
+                           mode=_abi.RENDER_WAVEFRONT) for d in datas]
+    films = [torch.empty((d.height, d.width, 4), dtype=torch.float32, device="cuda") for d in datas]
+    _, st = ab.render_batch(objs, opts, films)                  # autotune + warm-up
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        _, st = ab.render_batch(objs, opts, films)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    for o in objs:
+        o.close()
+    paths = sum(d.width * d.height * d.render["spp"] for d in datas)
+    return {"workload": "64 box scenes (seed 6+i), 128^2..512^2, 4/16/64 spp, depth 3/5/8, one wavefront launch",
+            "paths": paths, "ms": ms, "value": paths / (ms / 1000.0), "unit": "path samples/s",
+            "wavefront_config": st["wf_config"], "launches": st["launches"]}
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -485,6 +512,7 @@ def main():
                "includes": "scene upload + device BVH build + render + film download"}
 
     adj = None if args.small else adjoint_ratio(ab, _abi, torch, ctx, stream)
+    batch = None if args.small else batch_timing(ab, _abi, torch, ctx, stream)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -513,7 +541,7 @@ def main():
                 "rays_per_s": world * rays_step / (ms_step / 1000.0), "kernel_ms_per_step": kms_step,
                 "host_ms_per_call": st.get("host_ms_per_call"),
                 "bvh_build_s": build_s, "gpu_launches": launches, "roofline": roof, "cpu_baseline": cpu,
-                "e2e": e2e, "clocks": clk, "adjoint_forward": adj}
+                "e2e": e2e, "clocks": clk, "adjoint_forward": adj, "batch64": batch}
         line.update(other)
         print(json.dumps(line), flush=True)
     scene.close()
