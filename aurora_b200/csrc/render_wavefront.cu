@@ -156,7 +156,7 @@ __global__ void k_regen(WfPool w, int in_q) {
             // plain kernel's order of operations (integrate_direct)
             const uint32_t vis = w.sh_vis[i];
             const float4 c0 = w.sh_c0[i], c1 = w.sh_c1[i], t = w.sh_t[i];
-            const float nvis = w.sh_p[i].w;
+            const float nvis = t.w;   // the number of visible lights rides in the throughput record
             float3 res = mk(0.f, 0.f, 0.f);
             if (vis & 1u) res += mk(c0.x, c0.y, c0.z);
             if (vis & 2u) res += mk(c1.x, c1.y, c1.z);
@@ -489,12 +489,12 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                         }
                         if (r0 || r1) {
                             if (kRec) w.rec_cur[slot] = rec_at;
-                            w.sh_p[slot] = make_float4(f.P.x, f.P.y, f.P.z, (float)nvis);
+                            w.sh_p[slot] = make_float4(f.P.x, f.P.y, f.P.z, 0.f);
                             w.sh_d0[slot] = make_float4(d0.x, d0.y, d0.z, m0);
                             w.sh_d1[slot] = make_float4(d1.x, d1.y, d1.z, m1);
                             w.sh_c0[slot] = make_float4(c0.x, c0.y, c0.z, 0.f);
                             w.sh_c1[slot] = make_float4(c1.x, c1.y, c1.z, 0.f);
-                            w.sh_t[slot] = make_float4(T.x, T.y, T.z, 0.f);
+                            w.sh_t[slot] = make_float4(T.x, T.y, T.z, (float)nvis);
                             w.sh_vis[slot] = 0u;
                             push_sh0 = r0;
                             push_sh1 = r1;
