@@ -65,3 +65,13 @@ def test_record_layouts():
     assert C.sizeof(_abi.Hit) == 20
     assert C.sizeof(_abi.RenderOpts) == 48
     assert C.sizeof(_abi.RenderStats) == 136
+
+
+def test_accelerator_adapter_driver_links(built):
+    """The compiled AccelerationStructure adapter (aurora_b200/adapters) and its C++ driver are
+    built beside the library and link against it: without arguments the driver prints its usage
+    and exits 2 before touching a GPU."""
+    exe = os.path.join(os.path.dirname(built), "test_gpu_accelerator")
+    assert os.path.exists(exe)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 2 and "usage" in r.stderr
