@@ -381,7 +381,10 @@ __device__ __forceinline__ void flush_block(const float* s_g, const float* s_c, 
 // Megakernel form: one thread per pixel runs, for each of its camera samples, pass 1
 // (forward with tracing, records in thread-local memory) and pass 2 of each path. With
 // light samples a camera sample's n paths start at its camera ray's first hit (traced
-// once) and draw from sample indices s * L + j (integrate_camera_sample).
+// once) and draw from sample indices s * L + j (integrate_camera_sample). kMulti: light
+// samples above one; the one-path form keeps a single path per sample (no inner loop), whose
+// code is smaller and faster.
+template <bool kMulti>
 __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p, const float4* __restrict__ dfilm,
                                                        int nmat, float* g_mat, float* g_mat_c, float* g_tex,
                                                        float* g_tex_c, unsigned long long* counters) {
@@ -390,10 +393,11 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
     __syncthreads();
     const int npix = sc.cam.w * sc.cam.h;
     const int pixel = blockIdx.x * blockDim.x + threadIdx.x;
-    const int lmax = p.light_samples > 1 ? p.light_samples : 1;
+    const int lmax = kMulti && p.light_samples > 1 ? p.light_samples : 1;
     RayCounts rc;
     MatCache mc;
-    uint32_t paths = 0;
+    // paths traced for this pixel: the render's sample 0 has one, every other sample lmax
+    const uint32_t paths = pixel < npix ? (uint32_t)(p.spp * lmax - (p.sample_offset == 0 ? lmax - 1 : 0)) : 0u;
     if (pixel < npix) {
         const float4 df = dfilm[pixel];
         const float inv = 1.f / (float)p.spp;
@@ -404,7 +408,7 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
         const bool any = delta.x != 0.f || delta.y != 0.f || delta.z != 0.f;
         for (int s = 0; any && s < p.spp; ++s) {
             const int pass = p.sample_offset + s;
-            const int n = pass == 0 ? 1 : lmax;
+            const int n = kMulti ? (pass == 0 ? 1 : lmax) : 1;
             cam_rng.base = path_base((uint32_t)pixel, (uint32_t)(pass * lmax));
             RayF ray0 = camera_ray(sc.cam, px, py, cam_rng.u(kDimCamera), cam_rng.u(kDimCamera + 1));
             const float3 cam_d = ray0.d;
@@ -415,7 +419,6 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
             for (int j = 0; j < n; ++j) {
                 PathRng rng = cam_rng;
                 rng.base = path_base((uint32_t)pixel, (uint32_t)(pass * lmax + j));
-                ++paths;
                 // ---------------- pass 1: forward, recording hits and visibility
                 float4 rec[kAdjMaxDepth];
                 int nv = 0;
@@ -608,9 +611,13 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
             if (e == cudaSuccess && cudaEventElapsedTime(&rms, er0, er1) == cudaSuccess) replay_ms += rms;
         }
     } else if (e == cudaSuccess) {
-        k_adjoint<<<(unsigned)((npix + kAdjBlock - 1) / kAdjBlock), kAdjBlock, 0, s>>>(
-            sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm, ntex ? (float*)gt.ptr : nullptr, ct,
-            sc->ctx->counters);
+        const unsigned grid = (unsigned)((npix + kAdjBlock - 1) / kAdjBlock);
+        if (p.light_samples > 1)
+            k_adjoint<true><<<grid, kAdjBlock, 0, s>>>(sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
+                                                       ntex ? (float*)gt.ptr : nullptr, ct, sc->ctx->counters);
+        else
+            k_adjoint<false><<<grid, kAdjBlock, 0, s>>>(sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
+                                                        ntex ? (float*)gt.ptr : nullptr, ct, sc->ctx->counters);
         ++launches;
         e = cudaGetLastError();
     }

@@ -51,26 +51,7 @@ __device__ __forceinline__ bool slab_nf(float nx, float fx, float ny, float fy, 
     return tn <= tf;
 }
 
-// Node records are read far more often than triangle records (every ray passes the top
-// levels) and the 4-wide tree of a large scene (36 MB at 3.4 M triangles) fits in the L2
-// beside a share of the triangles. With AUR_NODE_L2_HINT the node loads carry an L2
-// evict_last cache policy (createpolicy + ld.global.nc.L2::cache_hint), so the triangle
-// stream does not push the tree out of the L2.
-#ifndef AUR_NODE_L2_HINT
-#define AUR_NODE_L2_HINT 0
-#endif
-__device__ __forceinline__ float4 ld_node(const float4* a) {
-#if AUR_NODE_L2_HINT
-    uint64_t pol;
-    asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(pol));
-    float4 v;
-    asm("ld.global.nc.L2::cache_hint.v4.f32 {%0, %1, %2, %3}, [%4], %5;"
-        : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(a), "l"(pol));
-    return v;
-#else
-    return __ldg(a);
-#endif
-}
+__device__ __forceinline__ float4 ld_node(const float4* a) { return __ldg(a); }
 
 // The four children's near and far planes of a 4-wide node: loads the lo or hi
 // float4 of each axis by the direction's sign (lox, hix, loy, hiy, loz, hiz order).

@@ -38,6 +38,7 @@ def test_sphere_and_terrain_match_plain(ctx, kelemen_tables):
 
 
 def test_batch_matches_single_renders(ctx):
+    """12 scenes of the batch against their single renders on the same (4-wide) tree."""
     import aurora_b200 as ab
     from aurora_b200 import scenes, _abi
     datas = scenes.batch_scenes(12)
@@ -48,7 +49,7 @@ def test_batch_matches_single_renders(ctx):
     assert stats["paths"] == sum(d.width * d.height * d.render["spp"] for d in datas)
     for d, s, f in zip(datas, objs, films):
         alone = s.render(ab.render_opts(d.render["spp"], d.render["max_depth"], d.render["min_depth"],
-                                        d.render["seed"])).film
+                                        d.render["seed"], mode=_abi.RENDER_WAVEFRONT)).film
         np.testing.assert_allclose(f, alone, rtol=1e-6, atol=1e-7)
     for s in objs:
         s.close()
