@@ -464,7 +464,9 @@ def main():
                     "peak_kind": peak_kind, "algorithmic_frac": achieved / peak,
                     "dram_frac": traffic / (kms / 1000.0) / 1e9 / peak if traffic else None},
             "simt_lanes_per_inst": prof.get("lanes_per_inst"), "fma_pipe_pct": prof.get("fma_pipe_pct"),
-            "alu_pipe_pct": prof.get("alu_pipe_pct"), "profile": prof.get("source"),
+            "alu_pipe_pct": prof.get("alu_pipe_pct"), "l1tex_throughput_pct": prof.get("l1tex_throughput_pct"),
+            "lts_throughput_pct": prof.get("lts_throughput_pct"), "issue_active_pct": prof.get("issue_active_pct"),
+            "profile": prof.get("source"),
             "algorithmic_bytes_per_step": kbytes,
             "closest_bytes_per_path": closest_bpp, "shadow_bytes_per_path": shadow_bpp,
             "node_bytes": node_b,
