@@ -66,9 +66,18 @@ struct WfScene {
     float4* lo_raw;        // [items] unclamped path radiance, w = number of recorded vertices
 };
 
+// Per-slot state in 32-byte pairs (one DRAM sector per slot and pair), structure of arrays
+// over the slots: the stages gather slots in queue order (material buckets, not slot order),
+// so a float4 of its own array would pull a half-used sector per field; a pair of fields that
+// are read together fills its sector, and slot-order sweeps (regen) stay coalesced.
+//   ray    origin + mint, direction + maxt        (extend, shade; written by regen, shade)
+//   hitid  hit (t, u, v, prim), id (scene, pixel, sub-sample, flags)   (extend, sort, shade, regen)
+//   tplo   throughput + roulette factor, radiance + alpha              (shade, regen)
+//   neeA   shading point, first next-event direction + maxt            (shadow)
+//   neeB   second next-event direction + maxt, its contribution        (shadow, regen)
+//   neeC   first next-event contribution, throughput + nvis            (regen)
 struct WfPool {
-    float4 *ray_o, *ray_d, *tp, *lo, *hit, *sh_p, *sh_d0, *sh_d1, *sh_c0, *sh_c1, *sh_t;
-    uint4* id;
+    float4 *ray, *hitid, *tplo, *neeA, *neeB, *neeC;   // [P][2] each
     uint32_t* state;            // PS_* in the low bits, PS_PENDING when next-event rays are in flight
     uint32_t* sh_vis;           // bit k: next-event ray k of the slot is unoccluded
     uint32_t* rec_cur;          // record mode: record index of the vertex whose next-event rays are in flight
@@ -78,6 +87,18 @@ struct WfPool {
     const WfScene* scenes;
     int nscenes;                // table capacity; unused entries start at item UINT32_MAX
     uint32_t P;
+    __device__ __forceinline__ float4& ray_o(uint32_t i) const { return ray[2 * (size_t)i]; }
+    __device__ __forceinline__ float4& ray_d(uint32_t i) const { return ray[2 * (size_t)i + 1]; }
+    __device__ __forceinline__ float4& hit(uint32_t i) const { return hitid[2 * (size_t)i]; }
+    __device__ __forceinline__ uint4& id(uint32_t i) const { return reinterpret_cast<uint4*>(hitid)[2 * (size_t)i + 1]; }
+    __device__ __forceinline__ float4& tp(uint32_t i) const { return tplo[2 * (size_t)i]; }
+    __device__ __forceinline__ float4& lo(uint32_t i) const { return tplo[2 * (size_t)i + 1]; }
+    __device__ __forceinline__ float4& sh_p(uint32_t i) const { return neeA[2 * (size_t)i]; }
+    __device__ __forceinline__ float4& sh_d0(uint32_t i) const { return neeA[2 * (size_t)i + 1]; }
+    __device__ __forceinline__ float4& sh_d1(uint32_t i) const { return neeB[2 * (size_t)i]; }
+    __device__ __forceinline__ float4& sh_c1(uint32_t i) const { return neeB[2 * (size_t)i + 1]; }
+    __device__ __forceinline__ float4& sh_c0(uint32_t i) const { return neeC[2 * (size_t)i]; }
+    __device__ __forceinline__ float4& sh_t(uint32_t i) const { return neeC[2 * (size_t)i + 1]; }
 };
 
 // flags in id.w; kNoClamp: the sample is the environment seen by the camera ray, which
@@ -155,25 +176,25 @@ __global__ void k_regen(WfPool w, int in_q) {
             // next-event estimate of the last vertex: Lo += ((vis0 c0 + vis1 c1) nvis) T, the
             // plain kernel's order of operations (integrate_direct)
             const uint32_t vis = w.sh_vis[i];
-            const float4 c0 = w.sh_c0[i], c1 = w.sh_c1[i], t = w.sh_t[i];
+            const float4 t = w.sh_t(i);
             const float nvis = t.w;   // the number of visible lights rides in the throughput record
             float3 res = mk(0.f, 0.f, 0.f);
-            if (vis & 1u) res += mk(c0.x, c0.y, c0.z);
-            if (vis & 2u) res += mk(c1.x, c1.y, c1.z);
-            float4 lo = w.lo[i];
+            if (vis & 1u) { const float4 c0 = w.sh_c0(i); res += mk(c0.x, c0.y, c0.z); }   // only unoccluded
+            if (vis & 2u) { const float4 c1 = w.sh_c1(i); res += mk(c1.x, c1.y, c1.z); }   // contributions are read
+            float4 lo = w.lo(i);
             const float3 add = (res * nvis) * mk(t.x, t.y, t.z);
             lo.x += add.x; lo.y += add.y; lo.z += add.z;
-            w.lo[i] = lo;
+            w.lo(i) = lo;
             st &= ~PS_PENDING;
             if (kRec) {   // the visibility of the vertex's next-event rays goes into its record
-                float4* r = w.scenes[w.id[i].x].rec + w.rec_cur[i];
+                float4* r = w.scenes[w.id(i).x].rec + w.rec_cur[i];
                 r->w = __int_as_float(__float_as_int(r->w) | (int)(vis << 30));
             }
         }
         if (st == PS_DONE) {
-            const uint4 id = w.id[i];
+            const uint4 id = w.id(i);
             const WfScene& S = w.scenes[id.x];
-            const float4 lo = w.lo[i];
+            const float4 lo = w.lo(i);
             if (kRec) {
                 S.lo_raw[(size_t)id.z * S.npix + id.y] = make_float4(lo.x, lo.y, lo.z, __int_as_float(f_vtx(id.w)));
             } else {
@@ -211,11 +232,11 @@ __global__ void k_regen(WfPool w, int in_q) {
             rng.base = path_base(pixel, cam_index(S, q));
             const RayF r = camera_ray(S.sc.cam, (int)(pixel % (uint32_t)S.sc.cam.w), (int)(pixel / (uint32_t)S.sc.cam.w),
                                       rng.u(kDimCamera), rng.u(kDimCamera + 1));
-            w.ray_o[i] = make_float4(r.o.x, r.o.y, r.o.z, r.mint);
-            w.ray_d[i] = make_float4(r.d.x, r.d.y, r.d.z, r.maxt);
-            w.tp[i] = make_float4(1.f, 1.f, 1.f, 1.f);
-            w.lo[i] = make_float4(0.f, 0.f, 0.f, 0.f);
-            w.id[i] = make_uint4((uint32_t)s, pixel, q, pack_flags(0, 0, RAY_CAMERA, false));
+            w.ray_o(i) = make_float4(r.o.x, r.o.y, r.o.z, r.mint);
+            w.ray_d(i) = make_float4(r.d.x, r.d.y, r.d.z, r.maxt);
+            w.tp(i) = make_float4(1.f, 1.f, 1.f, 1.f);
+            w.lo(i) = make_float4(0.f, 0.f, 0.f, 0.f);
+            w.id(i) = make_uint4((uint32_t)s, pixel, q, pack_flags(0, 0, RAY_CAMERA, false));
             st = PS_ACTIVE;
         }
         {
@@ -284,11 +305,11 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
                 const uint32_t k = b + __popc(m & lanemask_lt());
                 if (k < n) {
                     slot = qin[k];
-                    S = &w.scenes[w.id[slot].x];
+                    S = &w.scenes[w.id(slot).x];
                     if constexpr (kWide) nodes = S->sc.nodes4;
                     else nodes = S->sc.nodes;
                     tris = S->sc.tris;
-                    const float4 o = w.ray_o[slot], d = w.ray_d[slot];
+                    const float4 o = w.ray_o(slot), d = w.ray_d(slot);
                     ts.begin(mk(o.x, o.y, o.z), mk(d.x, d.y, d.z), o.w, d.w);
                     has = true;
                 } else {
@@ -304,7 +325,7 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
         done = done && has;
         int bucket = -1;
         if (done) {
-            w.hit[slot] = make_float4(ts.tbest, ts.bu, ts.bv, __int_as_float(ts.best));
+            w.hit(slot) = make_float4(ts.tbest, ts.bu, ts.bv, __int_as_float(ts.best));
             if (kSort) bucket = bucket_of(S->sc.sh, ts.best);
             has = false;
         }
@@ -343,8 +364,8 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
         uint32_t slot = 0, local = 0;
         if (k < n) {
             slot = qin[k];
-            const int prim = __float_as_int(w.hit[slot].w);
-            bucket = bucket_of(w.scenes[w.id[slot].x].sc.sh, prim);
+            const int prim = __float_as_int(w.hit(slot).w);
+            bucket = bucket_of(w.scenes[w.id(slot).x].sc.sh, prim);
         }
         const uint32_t active = __ballot_sync(0xffffffffu, bucket >= 0);
         if (bucket >= 0) {
@@ -367,8 +388,8 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
 // A ray that missed in a scene with environment lights: the camera ray sees the
 // environment (alpha 1, no firefly filter), an escaping mirror ray adds it times the
 // throughput, both along the camera ray's direction (integrator.cpp:262-288). Out of line.
-__device__ __noinline__ float4 shade_env_miss(uint4* ids, const float4* tp, const WfScene* S, uint32_t slot, uint4 id,
-                                              int vtx, float4 lo) {
+__device__ __noinline__ float4 shade_env_miss(const WfPool* w, const WfScene* S, uint32_t slot, uint4 id, int vtx,
+                                              float4 lo) {
     PathRng rng;
     rng.key = S->key;
     rng.base = path_base(id.y, cam_index(*S, id.z));
@@ -376,10 +397,10 @@ __device__ __noinline__ float4 shade_env_miss(uint4* ids, const float4* tp, cons
                                rng.u(kDimCamera), rng.u(kDimCamera + 1));
     const float3 e = env_radiance_of(S->sc.sh.lights, S->sc.sh.nlights, S->sc.sh.texs, S->sc.sh.texels, cr.d);
     if (vtx == 0) {
-        ids[slot].w = id.w | kNoClamp;
+        w->id(slot).w = id.w | kNoClamp;
         return make_float4(e.x, e.y, e.z, 1.f);
     }
-    const float4 t = tp[slot];
+    const float4 t = w->tp(slot);
     const float3 a = e * mk(t.x, t.y, t.z);
     return make_float4(lo.x + a.x, lo.y + a.y, lo.z + a.z, lo.w);
 }
@@ -406,21 +427,21 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
         uint32_t slot = 0;
         if (k < n) {
             slot = qin[k];
-            const float4 hh = w.hit[slot];
+            const float4 hh = w.hit(slot);
             const int prim = __float_as_int(hh.w);
-            float4 lo = w.lo[slot];
+            float4 lo = w.lo(slot);
             if (prim < 0) {
-                const uint4 id = w.id[slot];
+                const uint4 id = w.id(slot);
                 const WfScene& S = w.scenes[id.x];
                 const int kind = f_kind(id.w), vtx = f_vtx(id.w);
                 if (S.sc.sh.nenv && (vtx == 0 || kind == RAY_MIRROR))
-                    lo = shade_env_miss(w.id, w.tp, &S, slot, id, vtx, lo);
+                    lo = shade_env_miss(&w, &S, slot, id, vtx, lo);
                 w.state[slot] = PS_DONE;
-            } else if (f_vtx(w.id[slot].w) >= w.scenes[w.id[slot].x].p.max_depth) {
+            } else if (f_vtx(w.id(slot).w) >= w.scenes[w.id(slot).x].p.max_depth) {
                 // the reference's unshaded last ray hit something: the path ends
                 w.state[slot] = PS_DONE;
             } else {
-                const uint4 id = w.id[slot];
+                const uint4 id = w.id(slot);
                 const WfScene& S = w.scenes[id.x];
                 const DevScene& sc = S.sc;
                 const uint32_t flags = id.w;
@@ -431,8 +452,8 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 PathRng rng;
                 rng.key = S.key;
                 rng.base = path_base(id.y, rng_index(S, id.z));
-                const float4 ro = w.ray_o[slot], rd = w.ray_d[slot];
-                float4 tpv = w.tp[slot];
+                const float4 ro = w.ray_o(slot), rd = w.ray_d(slot);
+                float4 tpv = w.tp(slot);
                 float3 T = mk(tpv.x, tpv.y, tpv.z);
                 float cont = tpv.w;
                 float3 Lo = mk(lo.x, lo.y, lo.z);
@@ -489,12 +510,12 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                         }
                         if (r0 || r1) {
                             if (kRec) w.rec_cur[slot] = rec_at;
-                            w.sh_p[slot] = make_float4(f.P.x, f.P.y, f.P.z, 0.f);
-                            w.sh_d0[slot] = make_float4(d0.x, d0.y, d0.z, m0);
-                            w.sh_d1[slot] = make_float4(d1.x, d1.y, d1.z, m1);
-                            w.sh_c0[slot] = make_float4(c0.x, c0.y, c0.z, 0.f);
-                            w.sh_c1[slot] = make_float4(c1.x, c1.y, c1.z, 0.f);
-                            w.sh_t[slot] = make_float4(T.x, T.y, T.z, (float)nvis);
+                            w.sh_p(slot) = make_float4(f.P.x, f.P.y, f.P.z, 0.f);
+                            w.sh_d0(slot) = make_float4(d0.x, d0.y, d0.z, m0);
+                            w.sh_d1(slot) = make_float4(d1.x, d1.y, d1.z, m1);
+                            w.sh_c0(slot) = make_float4(c0.x, c0.y, c0.z, 0.f);
+                            w.sh_c1(slot) = make_float4(c1.x, c1.y, c1.z, 0.f);
+                            w.sh_t(slot) = make_float4(T.x, T.y, T.z, (float)nvis);
                             w.sh_vis[slot] = 0u;
                             push_sh0 = r0;
                             push_sh1 = r1;
@@ -511,18 +532,18 @@ __global__ void k_shade(WfPool w, int in_q, int sorted) {
                 if (continue_path(brdf, bs, f.N, S.p.min_depth, rng, vtx, T, cont, kind, bounces) &&
                     (vtx + 1 < S.p.max_depth || (kind == RAY_MIRROR && sc.sh.nenv))) {
                     alive = true;
-                    w.ray_o[slot] = make_float4(f.P.x, f.P.y, f.P.z, kRayBias);
-                    w.ray_d[slot] = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.maxt);
-                    w.tp[slot] = make_float4(T.x, T.y, T.z, cont);
-                    w.id[slot].w = pack_flags(vtx + 1, bounces, kind, matte);
+                    w.ray_o(slot) = make_float4(f.P.x, f.P.y, f.P.z, kRayBias);
+                    w.ray_d(slot) = make_float4(bs.dir.x, bs.dir.y, bs.dir.z, bs.maxt);
+                    w.tp(slot) = make_float4(T.x, T.y, T.z, cont);
+                    w.id(slot).w = pack_flags(vtx + 1, bounces, kind, matte);
                 }
                 lo = make_float4(Lo.x, Lo.y, Lo.z, lo.w);
                 // a finished path's flags count its recorded vertices (a missed ray's vertex is not recorded)
-                if (kRec && !alive) w.id[slot].w = pack_flags(vtx + 1, bounces, kind, matte);
+                if (kRec && !alive) w.id(slot).w = pack_flags(vtx + 1, bounces, kind, matte);
                 w.state[slot] = (alive ? PS_ACTIVE : PS_DONE) | (push_sh0 || push_sh1 ? PS_PENDING : 0u);
                 push_ext = alive;
             }
-            w.lo[slot] = lo;
+            w.lo(slot) = lo;
         }
         {
             const bool pp[3] = {push_ext, push_sh0, push_sh1};
@@ -569,12 +590,12 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_shadow(WfPool w) {
                 if (k < n) {
                     entry = w.q_shadow[k];
                     const uint32_t slot = entry >> 1;
-                    const WfScene& S = w.scenes[w.id[slot].x];
+                    const WfScene& S = w.scenes[w.id(slot).x];
                     if constexpr (kWide) nodes = S.sc.nodes4;
                     else nodes = S.sc.nodes;
                     tris = S.sc.tris;
-                    const float4 p = w.sh_p[slot];
-                    const float4 d = (entry & 1u) ? w.sh_d1[slot] : w.sh_d0[slot];
+                    const float4 p = w.sh_p(slot);
+                    const float4 d = (entry & 1u) ? w.sh_d1(slot) : w.sh_d0(slot);
                     ts.begin(mk(p.x, p.y, p.z), mk(d.x, d.y, d.z), kRayBias, d.w);
                     has = true;
                 } else {
@@ -693,15 +714,14 @@ struct WfRun {
         cfg = c;
         stream = s;
         const size_t P = c.pool;
-        const size_t bytes = P * (11 * sizeof(float4) + sizeof(uint4) + 8 * sizeof(uint32_t)) + 20 * 256 +
+        const size_t bytes = P * (12 * sizeof(float4) + 8 * sizeof(uint32_t)) + 20 * 256 +
                              kCounters * sizeof(uint32_t) + 2 * sizeof(unsigned long long);
         cudaError_t e = cudaMalloc(&mem, bytes);
         if (e != cudaSuccess) return e;
         char* p = (char*)mem;
         auto take = [&](size_t n) { char* r = p; p += (n + 255) & ~(size_t)255; return (void*)r; };
-        float4** f4s[] = {&w.ray_o, &w.ray_d, &w.tp, &w.lo, &w.hit, &w.sh_p, &w.sh_d0, &w.sh_d1, &w.sh_c0, &w.sh_c1, &w.sh_t};
-        for (float4** q : f4s) *q = (float4*)take(P * sizeof(float4));
-        w.id = (uint4*)take(P * sizeof(uint4));
+        float4** pairs[] = {&w.ray, &w.hitid, &w.tplo, &w.neeA, &w.neeB, &w.neeC};
+        for (float4** q : pairs) *q = (float4*)take(2 * P * sizeof(float4));
         w.state = (uint32_t*)take(P * 4);
         w.q_ext0 = (uint32_t*)take(P * 4);
         w.q_ext1 = (uint32_t*)take(P * 4);
