@@ -130,7 +130,13 @@ DevScene aur_scene::dev() const {
     d.sh.texels = texels;
     d.sh.albedo = ctx->kelemen;
     d.sh.corner_n = corner_n;
-    d.sh.corner_uv = corner_uv;
+    // the per-corner uvs are read only where a uv-mapped shader (texture2DShader) needs them:
+    // a scene without one skips their 24 bytes per shaded vertex
+    bool uses_uv = false;
+    auto uv_tex = [&](int t) { return t >= 0 && t < (int)h_texs.size() && h_texs[t].tri_scale == 0.f; };
+    for (const Material& m : h_mats)
+        uses_uv = uses_uv || uv_tex(m.diff_tex) || uv_tex(m.spec_tex) || uv_tex(m.rough_tex) || uv_tex(m.norm_tex);
+    d.sh.corner_uv = uses_uv ? corner_uv : nullptr;
     d.sh.tri_attr = bvh.tri_attr;
     d.sh.nlights = (int)h_lights.size();
     d.sh.nenv = 0;
