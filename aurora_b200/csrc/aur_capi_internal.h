@@ -66,6 +66,8 @@ namespace aur {
 aur_status fail(aur_status s, const std::string& msg);
 aur_status cuda_fail(cudaError_t e, const char* where);
 bool is_device_ptr(const void* p);
+// Checks on the device that v[0, n) < bound (device pointer v); synchronises the stream.
+cudaError_t indices_below(const uint32_t* v, size_t n, uint32_t bound, bool* ok, cudaStream_t s);
 cudaError_t ctx_kelemen_ensure(aur_ctx* ctx, int refl_index);
 // The context's scratch buffer of at least `bytes` (kept and reused by later calls;
 // freed with the context). Work on the context's stream must not still use it.

@@ -4,6 +4,7 @@
 #include "aur_kernels.h"
 #include "aur_capi_internal.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -16,6 +17,38 @@ using namespace aur;
 namespace {
 thread_local std::string g_err;
 }
+
+namespace aur {
+// flag |= 1 when any of the n indices is >= bound (a grid-stride scan; stream-ordered, no sync)
+__global__ void k_check_below(const uint32_t* __restrict__ v, size_t n, uint32_t bound, uint32_t* flag) {
+    uint32_t bad = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+        bad |= v[i] >= bound ? 1u : 0u;
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(flag, 1u);
+}
+
+// Checks on the device that every index of v[0, n) is below bound (host or device inputs,
+// after their upload). Synchronises the stream. *ok = false on an index out of range.
+cudaError_t indices_below(const uint32_t* v, size_t n, uint32_t bound, bool* ok, cudaStream_t s) {
+    *ok = true;
+    if (n == 0) return cudaSuccess;
+    uint32_t* flag = nullptr;
+    cudaError_t e = cudaMallocAsync(&flag, sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(uint32_t), s);
+    if (e == cudaSuccess) {
+        const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, 148 * 8);
+        k_check_below<<<grid, 256, 0, s>>>(v, n, bound, flag);
+        e = cudaGetLastError();
+    }
+    uint32_t h = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, flag, sizeof(uint32_t), cudaMemcpyDeviceToHost, s);
+    if (flag) cudaFreeAsync(flag, s);
+    const cudaError_t se = cudaStreamSynchronize(s);
+    if (e == cudaSuccess) e = se;
+    *ok = h == 0;
+    return e;
+}
+}  // namespace aur
 
 namespace aur {
 aur_status fail(aur_status s, const std::string& msg) {
@@ -220,14 +253,14 @@ aur_status aur_bvh_build(aur_ctx* ctx, const float* verts, uint32_t nvert, const
     if (st != AUR_OK) return st;
     DeviceGuard g(ctx->device);
     cudaStream_t s = ctx->stream;
-    // vertex indices must be in range: checked on the host copy (device inputs are trusted)
-    if (!is_device_ptr(tri_vidx)) {
-        for (size_t k = 0; k < 3 * (size_t)ntri; ++k)
-            if (tri_vidx[k] >= nvert) return fail(AUR_ERR_INVALID_ARG, "aur_bvh_build: vertex index out of range");
-    }
     DevIn dv, di, da;
     CUDA_TRY(dv.init(verts, sizeof(float) * 3 * nvert, 4, s), "aur_bvh_build(upload)");
     CUDA_TRY(di.init(tri_vidx, sizeof(uint32_t) * 3 * ntri, 4, s), "aur_bvh_build(upload)");
+    // vertex indices must be in range before any build kernel reads vertices through them:
+    // checked on the device copy (host and device inputs alike)
+    bool in_range = true;
+    CUDA_TRY(indices_below((const uint32_t*)di.ptr, 3 * (size_t)ntri, nvert, &in_range, s), "aur_bvh_build(check)");
+    if (!in_range) return fail(AUR_ERR_INVALID_ARG, "aur_bvh_build: vertex index out of range");
     aur_bvh* b = new aur_bvh();
     b->ctx = ctx;
     cudaError_t e = bvh_build_device((const float*)dv.ptr, (const uint32_t*)di.ptr, (int)ntri, bo, &b->bvh, s);

@@ -162,12 +162,8 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     if (d->width <= 0 || d->height <= 0 || (long long)d->width * d->height > (1ll << 31) / 4)
         return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: bad resolution");
     if (d->ntex && (!d->tex_dims || !d->texels)) return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: textures missing");
-    // host-side validation of indices (device-resident inputs are trusted)
-    const bool host_attr = !is_device_ptr(d->tri_attr);
-    if (host_attr)
-        for (uint32_t i = 0; i < d->ntri; ++i)
-            if (d->tri_attr[i] < 0 || (uint32_t)d->tri_attr[i] >= d->nattr)
-                return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: triangle attribute out of range");
+    // the triangles' attribute indices are checked on the device after their upload (below);
+    // the attributes' material indices here (device-resident attribute tables are trusted)
     for (uint32_t i = 0; i < d->nattr; ++i)
         if (!is_device_ptr(d->attr_material) && (d->attr_material[i] < 0 || (uint32_t)d->attr_material[i] >= d->nmat))
             return fail(AUR_ERR_INVALID_ARG, "aur_scene_create: attribute material out of range");
@@ -245,6 +241,13 @@ aur_status aur_scene_create(aur_ctx* ctx, const aur_scene_desc* d, const aur_bvh
     }
     aur_bvh* tmp = nullptr;
     aur_status st = aur_bvh_build(ctx, d->verts, d->nvert, d->tri_vidx, d->tri_attr, d->ntri, bvh_opts, &tmp);
+    if (st == AUR_OK) {   // every triangle's attribute index below nattr (negative ones wrap above)
+        bool in_range = true;
+        const cudaError_t ce = indices_below((const uint32_t*)tmp->tri_attr, d->ntri, d->nattr, &in_range, s);
+        if (ce != cudaSuccess) st = cuda_fail(ce, "aur_scene_create(check)");
+        else if (!in_range) st = fail(AUR_ERR_INVALID_ARG, "aur_scene_create: triangle attribute out of range");
+        if (st != AUR_OK) { aur_bvh_destroy(tmp); tmp = nullptr; }
+    }
     if (uploader.joinable()) uploader.join();
     if (us) cudaStreamDestroy(us);
     if (st != AUR_OK) {
