@@ -219,3 +219,32 @@ def test_bvh_intersect_rejects_missing_shading(ctx):
     sb = scene.bvh()
     assert _abi.lib().aur_bvh_set_shading(sb.handle, n.ctypes.data, None) == _abi.ERR_INVALID_ARG
     scene.close()
+
+
+def test_indices_out_of_range_are_refused(ctx):
+    """Vertex indices (aur_bvh_build) and triangle attribute indices (aur_scene_create) are checked
+    on the device after their upload, host and device inputs alike, before any kernel reads
+    through them."""
+    import copy
+    import ctypes as C
+    import torch
+    import aurora_b200 as ab
+    from aurora_b200 import _abi, scenes
+    v = np.array([[0, 0, -2], [1, 0, -2], [0, 1, -2]], np.float32)
+    host = np.array([[0, 1, 3]], np.uint32)
+    dev = torch.tensor([[0, 1, 3]], dtype=torch.int32, device="cuda")
+    for ptr in (host.ctypes.data, dev.data_ptr()):
+        h = C.c_void_p()
+        st = _abi.lib().aur_bvh_build(ctx.handle, v.ctypes.data, 3, ptr, None, 1, None, C.byref(h))
+        assert st == _abi.ERR_INVALID_ARG and b"vertex index" in _abi.lib().aur_last_error()
+    data = scenes.box_scene(16, 16)
+    for bad in (-1, len(data.attr_material)):
+        d = copy.copy(data)
+        d.tri_attr = data.tri_attr.copy()
+        d.tri_attr[5] = bad
+        with pytest.raises(ab.AuroraError) as e:
+            ab.Scene(ctx, d)
+        assert e.value.status == _abi.ERR_INVALID_ARG and "attribute" in str(e.value)
+    ok = ab.Scene(ctx, data)                     # the context stays usable
+    assert ok.render(ab.render_opts(1, 5, 5, 1)).stats["paths"] == 256
+    ok.close()
