@@ -628,6 +628,13 @@ cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
     int2 *fa = nullptr, *fb = nullptr;
     int* counters = nullptr;
     CK(dalloc(&b->nodes4, cap, s));
+    // every 4-wide node must start on a 128-byte line (the traversals read it in 32-byte and
+    // 16-byte vector loads): the allocator's alignment, checked rather than assumed
+    if ((uintptr_t)b->nodes4 % sizeof(BvhNode4) != 0) {
+        cudaFreeAsync(b->nodes4, s);
+        b->nodes4 = nullptr;
+        return cudaErrorMisalignedAddress;
+    }
     CK(dalloc(&fa, cap, s));
     CK(dalloc(&fb, cap, s));
     CK(dalloc(&counters, 2, s));

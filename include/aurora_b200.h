@@ -245,7 +245,7 @@ typedef struct aur_render_opts {
     int32_t mode;           /* AUR_RENDER_PLAIN or AUR_RENDER_WAVEFRONT */
     int32_t fp64_film;      /* plain mode: accumulate in FP64 */
     int32_t wf_pool;        /* wavefront path-pool size, 0 = tuned/default */
-    int32_t wf_block;       /* wavefront block size, 0 = tuned/default */
+    int32_t wf_block;       /* wavefront block size (64, 128 or 256), 0 = tuned/default */
     int32_t wf_sort;        /* wavefront material sort: -1 tuned, 0 off, 1 on */
     int32_t count_work;     /* also count BVH node visits / triangle tests (slower; for profiling) */
     int32_t light_samples;  /* lightsamples (Integrator::integrateCameraSample's numSamples,

@@ -59,7 +59,7 @@ def test_invalid_wavefront_configs(ctx):
     import aurora_b200 as ab
     from aurora_b200 import scenes, _abi
     scene = ab.Scene(ctx, scenes.box_scene(16, 16))
-    for bad in (dict(wf_pool=1000), dict(wf_block=100), dict(wf_pool=1 << 27)):
+    for bad in (dict(wf_pool=1000), dict(wf_block=100), dict(wf_block=512), dict(wf_pool=1 << 27)):
         with pytest.raises(ab.AuroraError):
             scene.render(ab.render_opts(1, 5, 5, 1, mode=_abi.RENDER_WAVEFRONT, **bad))
 
