@@ -444,26 +444,23 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
                         if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
-                        if (vtx + 1 >= p.max_depth) {
-                            // the reference's unshaded last ray: an escaping mirror ray adds the
-                            // environment (integrator.cpp:256-274); replay sees it inside Lo
-                            if (kind == RAY_MIRROR && sc.sh.nenv) {
-                                ++rc.closest;
-                                if (!bvh_occluded(sc.nodes, sc.tris, f.P, bs.dir, kRayBias, bs.maxt, rc.work))
-                                    Lo += env_radiance(sc.sh, cam_d) * T;
-                            }
-                            break;
-                        }
+                        // the reference's unshaded last ray: only an escaping mirror ray adds
+                        // anything, the environment (integrator.cpp:256-274); replay sees it in Lo
+                        const bool last = vtx + 1 >= p.max_depth;
+                        if (last && !(kind == RAY_MIRROR && sc.sh.nenv)) break;
                         ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
                         ++rc.closest;
                         if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
                             if (kind == RAY_MIRROR && sc.sh.nenv) Lo += env_radiance(sc.sh, cam_d) * T;
                             break;
                         }
+                        if (last) break;
                     }
                 }
                 // ---------------- pass 2: re-shade the recorded vertices, accumulate gradients
-                replay_path(sc, p, px, py, cam_rng, rng, rec, nv, Lo, dn, mc, s_g, s_c, g_tex, g_tex_c, rc);
+                // one path per sample: its own generator drew the camera ray (cam_rng is no longer live)
+                replay_path(sc, p, px, py, kMulti ? cam_rng : rng, rng, rec, nv, Lo, dn, mc, s_g, s_c, g_tex,
+                            g_tex_c, rc);
             }
         }
     }

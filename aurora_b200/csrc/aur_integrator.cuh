@@ -12,8 +12,7 @@
 // shaded vertex; its hit is never shaded, and when it misses it adds the
 // environment lights if it is a mirror ray (:256-274). That ray is traced here
 // only when it can add something (a mirror ray in a scene with an environment
-// light), as an occlusion query over the same interval: whether it misses is
-// all that matters.
+// light); its hit ends the path unshaded.
 #pragma once
 #include "aur_traverse.cuh"
 
@@ -181,16 +180,11 @@ __device__ __forceinline__ float3 path_from_hit(const DevScene& sc, const PathPa
         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
         if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
-        if (vtx + 1 >= p.max_depth) {
-            // the reference's unshaded last ray (integrator.cpp:256-274): an escaping mirror
-            // ray sees the environment along the camera ray's direction
-            if (kind == RAY_MIRROR && sc.sh.nenv) {
-                ++rc.closest;
-                if (!trace_occluded<kWidth>(sc, f.P, bs.dir, kRayBias, bs.maxt, rc.work))
-                    Lo += env_radiance(sc.sh, cam_d) * T;
-            }
-            break;
-        }
+        // after the last vertex the reference traces one more ray whose hit is never shaded and
+        // whose miss adds the environment for a mirror ray (integrator.cpp:256-274): traced here
+        // only when it can add something, through the same call as every other ray
+        const bool last = vtx + 1 >= p.max_depth;
+        if (last && !(kind == RAY_MIRROR && sc.sh.nenv)) break;
         ray.o = f.P;
         ray.d = bs.dir;
         ray.mint = kRayBias;
@@ -202,6 +196,7 @@ __device__ __forceinline__ float3 path_from_hit(const DevScene& sc, const PathPa
             if (kind == RAY_MIRROR && sc.sh.nenv) Lo += env_radiance(sc.sh, cam_d) * T;
             break;
         }
+        if (last) break;
     }
     return firefly_clamp(Lo);
 }

@@ -80,3 +80,22 @@ def test_autotuned_config(ctx):
     np.testing.assert_allclose(a.film, plain.film, rtol=1e-6, atol=1e-7)
     assert sum(a.stats["stage_ms"].values()) > 0
     scene.close()
+
+
+def test_batch_with_light_samples(ctx):
+    """Scenes of one batch may use different light_samples: each film equals its single
+    wavefront render."""
+    import aurora_b200 as ab
+    from aurora_b200 import scenes, _abi
+    datas = [scenes.box_scene(64, 64, spp=6), scenes.sphere_scene(48, 48, spp=5), scenes.box_scene(32, 48, spp=4)]
+    ls = [1, 3, 2]
+    objs = [ab.Scene(ctx, d) for d in datas]
+    opts = [ab.render_opts(d.render["spp"], d.render["max_depth"], d.render["min_depth"], d.render["seed"],
+                           mode=_abi.RENDER_WAVEFRONT, light_samples=l) for d, l in zip(datas, ls)]
+    films, stats = ab.render_batch(objs, opts)
+    want = sum(d.width * d.height * (d.render["spp"] * l - (l - 1)) for d, l in zip(datas, ls))
+    assert stats["paths"] == want
+    for s, o, f in zip(objs, opts, films):
+        np.testing.assert_allclose(f, s.render(o).film, rtol=1e-6, atol=1e-7)
+    for s in objs:
+        s.close()
