@@ -378,13 +378,25 @@ __device__ __forceinline__ void flush_block(const float* s_g, const float* s_c, 
     }
 }
 
+// The environment seen by a mirror ray traced after the last shaded vertex (zero when the ray
+// hits anything in [RAY_BIAS, maxt]); out of line, as the case is rare.
+__device__ __noinline__ float3 escape_after_last(const BvhNode* nodes, const BvhTri* tris, const Light* lights,
+                                                 int nlights, const Texture* texs, const float* texels, float3 P,
+                                                 float3 dir, float maxt, float3 cam_d) {
+    TraceWork w;
+    if (bvh_occluded(nodes, tris, P, dir, kRayBias, maxt, w)) return mk(0.f, 0.f, 0.f);
+    return env_radiance_of(lights, nlights, texs, texels, cam_d);
+}
+
 // Megakernel form: one thread per pixel runs, for each of its camera samples, pass 1
 // (forward with tracing, records in thread-local memory) and pass 2 of each path. With
 // light samples a camera sample's n paths start at its camera ray's first hit (traced
 // once) and draw from sample indices s * L + j (integrate_camera_sample). kMulti: light
 // samples above one; the one-path form keeps a single path per sample (no inner loop), whose
-// code is smaller and faster.
-template <bool kMulti>
+// code is smaller and faster. kEnv: the scene has an environment light; only then is the ray
+// after the last vertex traced (any code for it in the loop made the kernel 8% slower on
+// scenes without one).
+template <bool kMulti, bool kEnv>
 __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p, const float4* __restrict__ dfilm,
                                                        int nmat, float* g_mat, float* g_mat_c, float* g_tex,
                                                        float* g_tex_c, unsigned long long* counters) {
@@ -444,17 +456,24 @@ __global__ void __launch_bounds__(kAdjBlock) k_adjoint(DevScene sc, PathParams p
                         const BrdfSample bs = brdf_sample(brdf, f.V, f.N, rng.u(vertex_dim(vtx, kDimBrdf)),
                                                           rng.u(vertex_dim(vtx, kDimBrdf + 1)));
                         if (!continue_path(brdf, bs, f.N, p.min_depth, rng, vtx, T, cont, kind, bounces)) break;
-                        // the reference's unshaded last ray: only an escaping mirror ray adds
-                        // anything, the environment (integrator.cpp:256-274); replay sees it in Lo
-                        const bool last = vtx + 1 >= p.max_depth;
-                        if (last && !(kind == RAY_MIRROR && sc.sh.nenv)) break;
+                        if (vtx + 1 >= p.max_depth) {
+                            // the reference's unshaded last ray: only an escaping mirror ray adds
+                            // anything, the environment (integrator.cpp:256-274); replay sees it in Lo
+                            if constexpr (kEnv) {
+                                if (kind == RAY_MIRROR) {
+                                    ++rc.closest;
+                                    Lo += escape_after_last(sc.nodes, sc.tris, sc.sh.lights, sc.sh.nlights,
+                                                            sc.sh.texs, sc.sh.texels, f.P, bs.dir, bs.maxt, cam_d) * T;
+                                }
+                            }
+                            break;
+                        }
                         ray.o = f.P; ray.d = bs.dir; ray.mint = kRayBias; ray.maxt = bs.maxt;
                         ++rc.closest;
                         if (!bvh_closest(sc.nodes, sc.tris, ray.o, ray.d, ray.mint, ray.maxt, &h, rc.work)) {
-                            if (kind == RAY_MIRROR && sc.sh.nenv) Lo += env_radiance(sc.sh, cam_d) * T;
+                            if (kEnv && kind == RAY_MIRROR) Lo += env_radiance(sc.sh, cam_d) * T;
                             break;
                         }
-                        if (last) break;
                     }
                 }
                 // ---------------- pass 2: re-shade the recorded vertices, accumulate gradients
@@ -609,12 +628,11 @@ extern "C" aur_status aur_render_adjoint(aur_scene* sc, const aur_render_opts* o
         }
     } else if (e == cudaSuccess) {
         const unsigned grid = (unsigned)((npix + kAdjBlock - 1) / kAdjBlock);
-        if (p.light_samples > 1)
-            k_adjoint<true><<<grid, kAdjBlock, 0, s>>>(sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
-                                                       ntex ? (float*)gt.ptr : nullptr, ct, sc->ctx->counters);
-        else
-            k_adjoint<false><<<grid, kAdjBlock, 0, s>>>(sc->dev(), p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
-                                                        ntex ? (float*)gt.ptr : nullptr, ct, sc->ctx->counters);
+        const DevScene dsc = sc->dev();
+        auto kern = p.light_samples > 1 ? (dsc.sh.nenv ? k_adjoint<true, true> : k_adjoint<true, false>)
+                                        : (dsc.sh.nenv ? k_adjoint<false, true> : k_adjoint<false, false>);
+        kern<<<grid, kAdjBlock, 0, s>>>(dsc, p, (const float4*)din.ptr, nmat, (float*)gm.ptr, cm,
+                                        ntex ? (float*)gt.ptr : nullptr, ct, sc->ctx->counters);
         ++launches;
         e = cudaGetLastError();
     }
