@@ -411,18 +411,23 @@ AUR_HD float kelemen_albedo(const float* table, float costheta, float roughness)
 // roughness * (1 - CAUSTIC_BLUR) + CAUSTIC_BLUR with the reference's double constants
 AUR_HD float caustic_blur(float r) { return (float)((double)r * (1.0 - 0.2) + 0.2); }
 
+// The Lambert lobe of a matte material (shading/materials/matteMaterial.h): its diffuse
+// colour or texture.
+AUR_HD Brdf matte_brdf(const ShadeScene& s, const Material& m, const Frame& f) {
+    Brdf b;
+    b.lobe = LOBE_MATTE;
+    b.color = m.diff_tex >= 0 ? shader_color(s, m.diff_tex, f) : m.diff;
+    b.rough = 0.f;
+    return b;
+}
+
 // Material::getBrdf for every supported material at shading point `f`. `lobe_u` is the
 // vertex's lobe-choice random number.
 AUR_HD Brdf get_brdf(const ShadeScene& s, int mat_id, const Frame& f, bool matte_path, float lobe_u) {
     const float3 V = f.V, N = f.N;
     Material m = s.mats[mat_id];
     Brdf b;
-    if (m.type == MAT_MATTE) {
-        b.lobe = LOBE_MATTE;
-        b.color = m.diff_tex >= 0 ? shader_color(s, m.diff_tex, f) : m.diff;
-        b.rough = 0.f;
-        return b;
-    }
+    if (m.type == MAT_MATTE) return matte_brdf(s, m, f);
     if (m.type == MAT_KELEMEN || m.type == MAT_COOKTORRANCE) {
         float rough = m.rough_tex >= 0 ? shader_float(s, m.rough_tex, f) : m.rough;
         if (matte_path) rough = caustic_blur(rough);

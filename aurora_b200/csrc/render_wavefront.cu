@@ -46,7 +46,7 @@ enum : int { B_MISS = 0, B_MATTE = 1, B_KELEMEN = 2, B_CT = 3, B_METAL = 4, B_CO
 // counters
 enum : int {
     C_EXT0 = 0, C_EXT1 = 1, C_SHADOW = 2, C_WORK = 3, C_TOTAL = 4, C_CUR_EXT = 5, C_CUR_SHADE = 6,
-    C_CUR_SHADOW = 7, C_CUR_SORT = 8, C_BUCKET = 16, C_FILL = 24, kCounters = 32
+    C_CUR_SHADOW = 7, C_CUR_SORT = 8, C_CUR_SHADE2 = 9, C_BUCKET = 16, C_FILL = 24, kCounters = 32
 };
 
 struct WfScene {
@@ -270,11 +270,12 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
     const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
     // Outputs of the later stages start empty. Only counters that no block of
     // this kernel touches are reset here; the bucket counters this kernel
-    // increments were reset by the previous shade (or the pass start).
+    // increments were reset by the previous next-event stage (or the pass start).
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         w.ctr[in_q ? C_EXT0 : C_EXT1] = 0;
         w.ctr[C_SHADOW] = 0;
         w.ctr[C_CUR_SHADE] = 0;
+        w.ctr[C_CUR_SHADE2] = 0;
         w.ctr[C_CUR_SHADOW] = 0;
         w.ctr[C_CUR_SORT] = 0;
         w.rays[0] += n;
@@ -407,20 +408,28 @@ __device__ __noinline__ float4 shade_env_miss(const WfPool* w, const WfScene* S,
 
 // Three resident 256-thread blocks per SM (85 registers, some spilled) instead of the two that
 // its 106 registers allow: 50.7 vs 52.3 ms per 1080p frame.
-template <bool kRec>
-__global__ void __launch_bounds__(256, 3) k_shade(WfPool w, int in_q, int sorted) {
+// kPart selects the entries: SHADE_ALL every queued one; with the queue sorted by bucket,
+// SHADE_MATTE the matte bucket alone (its lobe known at compile time, so the glossy lobes'
+// code and registers drop out) and SHADE_REST all others. The bucket counts stay in place
+// until the next-event stage resets them, after both parts have read them.
+enum : int { SHADE_ALL = 0, SHADE_MATTE = 1, SHADE_REST = 2 };
+#ifndef AUR_SHADE_MATTE_MINB
+#define AUR_SHADE_MATTE_MINB 4
+#endif
+template <bool kRec, int kPart>
+__global__ void __launch_bounds__(256, kPart == SHADE_MATTE ? AUR_SHADE_MATTE_MINB : 3) k_shade(WfPool w, int in_q, int sorted) {
     const uint32_t* qin = sorted ? w.q_sort : (in_q ? w.q_ext1 : w.q_ext0);
-    const uint32_t n = w.ctr[in_q ? C_EXT1 : C_EXT0];
+    const uint32_t n_all = w.ctr[in_q ? C_EXT1 : C_EXT0];
+    // the sorted queue holds the misses first, then the matte bucket
+    const uint32_t lo = kPart == SHADE_ALL ? 0u : w.ctr[C_BUCKET + B_MISS];
+    const uint32_t nm = kPart == SHADE_ALL ? 0u : w.ctr[C_BUCKET + B_MATTE];
+    const uint32_t n = kPart == SHADE_ALL ? n_all : kPart == SHADE_MATTE ? nm : n_all - nm;
     uint32_t* qout = in_q ? w.q_ext0 : w.q_ext1;
     uint32_t* cout = &w.ctr[in_q ? C_EXT0 : C_EXT1];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {   // extend and scatter are finished: reset their counters
-        w.ctr[C_CUR_EXT] = 0;
-        for (int k = 0; k < kBuckets; ++k) { w.ctr[C_BUCKET + k] = 0; w.ctr[C_FILL + k] = 0; }
-    }
     __shared__ BlockScan s_scan;
     __shared__ uint32_t s_fetch;
     while (true) {
-        if (threadIdx.x == 0) s_fetch = atomicAdd(&w.ctr[C_CUR_SHADE], blockDim.x);
+        if (threadIdx.x == 0) s_fetch = atomicAdd(&w.ctr[kPart == SHADE_MATTE ? C_CUR_SHADE2 : C_CUR_SHADE], blockDim.x);
         __syncthreads();
         const uint32_t b = s_fetch;   // rewritten only after block_reserve's barriers below
         if (b >= n) break;
@@ -428,7 +437,7 @@ __global__ void __launch_bounds__(256, 3) k_shade(WfPool w, int in_q, int sorted
         bool push_ext = false, push_sh0 = false, push_sh1 = false;
         uint32_t slot = 0;
         if (k < n) {
-            slot = qin[k];
+            slot = qin[kPart == SHADE_ALL ? k : kPart == SHADE_MATTE ? lo + k : (k < lo ? k : k + nm)];
             const float4 hh = w.hit(slot);
             const int prim = __float_as_int(hh.w);
             float4 lo = w.lo(slot);
@@ -466,8 +475,9 @@ __global__ void __launch_bounds__(256, 3) k_shade(WfPool w, int in_q, int sorted
                 const Attr at = sc.sh.attrs[f.attr];
                 if (kind == RAY_DIFFUSE) matte = true;
                 if (collects_emission(kind)) Lo += T * at.emission;
-                const Brdf brdf = get_brdf(sc.sh, at.material, f, matte,
-                                           rng.u(vertex_dim(vtx, kDimLobe)));
+                const Brdf brdf = kPart == SHADE_MATTE
+                                      ? matte_brdf(sc.sh, sc.sh.mats[at.material], f)
+                                      : get_brdf(sc.sh, at.material, f, matte, rng.u(vertex_dim(vtx, kDimLobe)));
                 // next-event estimation: rays and their unoccluded contributions
                 if (brdf.lobe == LOBE_MATTE || brdf.lobe == LOBE_SPEC) {
                     int nvis;
@@ -568,7 +578,12 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_shadow(WfPool w) {
     using Trace = std::conditional_t<kWide, TraceState4<true>, TraceState<true>>;
     using Node = std::conditional_t<kWide, BvhNode4, BvhNode>;
     const uint32_t n = w.ctr[C_SHADOW];
-    if (blockIdx.x == 0 && threadIdx.x == 0) w.rays[1] += n;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        w.rays[1] += n;
+        // extend, scatter and shade are finished: reset their fetch and bucket counters
+        w.ctr[C_CUR_EXT] = 0;
+        for (int k = 0; k < kBuckets; ++k) { w.ctr[C_BUCKET + k] = 0; w.ctr[C_FILL + k] = 0; }
+    }
     extern __shared__ int s_stack[];
     Stack stack;
     stack.col = s_stack + threadIdx.x;
@@ -703,7 +718,7 @@ struct WfRun {
     size_t acc_bytes = 0;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t stream = nullptr;
-    int grid_regen = 0, grid_ext = 0, grid_shade = 0, grid_shadow = 0, grid_sort = 0;
+    int grid_regen = 0, grid_ext = 0, grid_shade = 0, grid_shade_m = 0, grid_shade_r = 0, grid_shadow = 0, grid_sort = 0;
     size_t stack_smem = 0;                     // shared traversal stack of one block
     uint32_t* h_ctr = nullptr;   // pinned
     static constexpr int kItersPerGraph = 8;
@@ -755,7 +770,9 @@ struct WfRun {
         const void* ext = c.wide ? (c.sort ? (const void*)k_extend<true, true> : (const void*)k_extend<false, true>)
                                  : (c.sort ? (const void*)k_extend<true, false> : (const void*)k_extend<false, false>);
         grid_ext = persist(ext, stack_smem);
-        grid_shade = persist(c.record ? (const void*)k_shade<true> : (const void*)k_shade<false>, 0);
+        grid_shade = persist(c.record ? (const void*)k_shade<true, SHADE_ALL> : (const void*)k_shade<false, SHADE_ALL>, 0);
+        grid_shade_m = persist(c.record ? (const void*)k_shade<true, SHADE_MATTE> : (const void*)k_shade<false, SHADE_MATTE>, 0);
+        grid_shade_r = persist(c.record ? (const void*)k_shade<true, SHADE_REST> : (const void*)k_shade<false, SHADE_REST>, 0);
         grid_shadow = persist(c.wide ? (const void*)k_shadow<true> : (const void*)k_shadow<false>, stack_smem);
         grid_sort = persist((const void*)k_sort_scatter, 0);
         grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 16);
@@ -779,8 +796,19 @@ struct WfRun {
         cudaEventRecordWithFlags(e[1], stream, cudaEventRecordExternal);
         if (cfg.sort) k_sort_scatter<<<grid_sort, cfg.block, 0, stream>>>(w, in_q);
         cudaEventRecordWithFlags(e[2], stream, cudaEventRecordExternal);
-        if (cfg.record) k_shade<true><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
-        else k_shade<false><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, cfg.sort);
+        if (cfg.sort) {   // the matte bucket, then the others
+            if (cfg.record) {
+                k_shade<true, SHADE_MATTE><<<grid_shade_m, cfg.block, 0, stream>>>(w, in_q, 1);
+                k_shade<true, SHADE_REST><<<grid_shade_r, cfg.block, 0, stream>>>(w, in_q, 1);
+            } else {
+                k_shade<false, SHADE_MATTE><<<grid_shade_m, cfg.block, 0, stream>>>(w, in_q, 1);
+                k_shade<false, SHADE_REST><<<grid_shade_r, cfg.block, 0, stream>>>(w, in_q, 1);
+            }
+        } else if (cfg.record) {
+            k_shade<true, SHADE_ALL><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, 0);
+        } else {
+            k_shade<false, SHADE_ALL><<<grid_shade, cfg.block, 0, stream>>>(w, in_q, 0);
+        }
         cudaEventRecordWithFlags(e[3], stream, cudaEventRecordExternal);
         if (cfg.wide) k_shadow<true><<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
         else k_shadow<false><<<grid_shadow, cfg.block, stack_smem, stream>>>(w);
@@ -797,7 +825,7 @@ struct WfRun {
         if (e != cudaSuccess) return e;
         e = cudaGraphInstantiate(&exec, g, 0);
         cudaGraphDestroy(g);
-        launches_per_graph = kItersPerGraph * (cfg.sort ? 5 : 4);
+        launches_per_graph = kItersPerGraph * (cfg.sort ? 6 : 4);
         return e;
     }
 
