@@ -171,30 +171,37 @@ __global__ void k_regen(WfPool w, int in_q) {
     for (uint32_t base = blockIdx.x * blockDim.x; base < w.P; base += stride) {
         const uint32_t i = base + threadIdx.x;
         const bool valid = i < w.P;
-        uint32_t st = valid ? w.state[i] : (uint32_t)PS_ACTIVE;
+        uint32_t st = PS_ACTIVE, vis = 0;
+        float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), t = lo, c0 = lo;
+        uint4 id = make_uint4(0, 0, 0, 0);
+        if (valid) {
+            // the slot's records are loaded together, before its state says which of them it
+            // uses, so that their latencies overlap (c0 and t share one 32-byte pair)
+            st = w.state[i];
+            vis = w.sh_vis[i];
+            t = w.sh_t(i);
+            c0 = w.sh_c0(i);
+            lo = w.lo(i);
+            id = w.id(i);
+        }
         if (st & PS_PENDING) {
             // next-event estimate of the last vertex: Lo += ((vis0 c0 + vis1 c1) nvis) T, the
             // plain kernel's order of operations (integrate_direct)
-            const uint32_t vis = w.sh_vis[i];
-            const float4 t = w.sh_t(i);
             const float nvis = t.w;   // the number of visible lights rides in the throughput record
             float3 res = mk(0.f, 0.f, 0.f);
-            if (vis & 1u) { const float4 c0 = w.sh_c0(i); res += mk(c0.x, c0.y, c0.z); }   // only unoccluded
-            if (vis & 2u) { const float4 c1 = w.sh_c1(i); res += mk(c1.x, c1.y, c1.z); }   // contributions are read
-            float4 lo = w.lo(i);
+            if (vis & 1u) res += mk(c0.x, c0.y, c0.z);   // only unoccluded contributions are added
+            if (vis & 2u) { const float4 c1 = w.sh_c1(i); res += mk(c1.x, c1.y, c1.z); }
             const float3 add = (res * nvis) * mk(t.x, t.y, t.z);
             lo.x += add.x; lo.y += add.y; lo.z += add.z;
             w.lo(i) = lo;
             st &= ~PS_PENDING;
             if (kRec) {   // the visibility of the vertex's next-event rays goes into its record
-                float4* r = w.scenes[w.id(i).x].rec + w.rec_cur[i];
+                float4* r = w.scenes[id.x].rec + w.rec_cur[i];
                 r->w = __int_as_float(__float_as_int(r->w) | (int)(vis << 30));
             }
         }
         if (st == PS_DONE) {
-            const uint4 id = w.id(i);
             const WfScene& S = w.scenes[id.x];
-            const float4 lo = w.lo(i);
             if (kRec) {
                 S.lo_raw[(size_t)id.z * S.npix + id.y] = make_float4(lo.x, lo.y, lo.z, __int_as_float(f_vtx(id.w)));
             } else {
