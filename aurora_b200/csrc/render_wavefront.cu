@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(256, kPart == SHADE_MATTE ? AUR_SHADE_MATTE_MI
     const uint32_t* qin = sorted ? w.q_sort : (in_q ? w.q_ext1 : w.q_ext0);
     const uint32_t n_all = w.ctr[in_q ? C_EXT1 : C_EXT0];
     // the sorted queue holds the misses first, then the matte bucket
-    const uint32_t lo = kPart == SHADE_ALL ? 0u : w.ctr[C_BUCKET + B_MISS];
+    const uint32_t nmiss = kPart == SHADE_ALL ? 0u : w.ctr[C_BUCKET + B_MISS];
     const uint32_t nm = kPart == SHADE_ALL ? 0u : w.ctr[C_BUCKET + B_MATTE];
     const uint32_t n = kPart == SHADE_ALL ? n_all : kPart == SHADE_MATTE ? nm : n_all - nm;
     uint32_t* qout = in_q ? w.q_ext0 : w.q_ext1;
@@ -444,7 +444,7 @@ __global__ void __launch_bounds__(256, kPart == SHADE_MATTE ? AUR_SHADE_MATTE_MI
         bool push_ext = false, push_sh0 = false, push_sh1 = false;
         uint32_t slot = 0;
         if (k < n) {
-            slot = qin[kPart == SHADE_ALL ? k : kPart == SHADE_MATTE ? lo + k : (k < lo ? k : k + nm)];
+            slot = qin[kPart == SHADE_ALL ? k : kPart == SHADE_MATTE ? nmiss + k : (k < nmiss ? k : k + nm)];
             const float4 hh = w.hit(slot);
             const int prim = __float_as_int(hh.w);
             float4 lo = w.lo(slot);
