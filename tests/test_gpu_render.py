@@ -214,3 +214,21 @@ def test_invalid_options(ctx):
                 ab.render_opts(4, 5, 5, 1, mode=7)):
         with pytest.raises(ab.AuroraError):
             scene.render(bad)
+
+
+@pytest.mark.parametrize("rough", [0.15, 0.4])
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_ct_direct_lighting_known_answer(ctx, mode, rough):
+    """Glossy next-event estimation with MIS on the device against the closed-form expectation
+    of the reference's estimator (the sampler's N.H > 0.999 cap included). Every pixel of the
+    16 x 16 film sees the same point at fov slope 1e-4, so the pixels are independent
+    estimates of one value and their spread gives the standard error."""
+    import aurora_b200 as ab
+    from test_oracle import ct_plane_under_light
+    data, want, plain = ct_plane_under_light(rough)
+    spp = 16384
+    res = ab.Scene(ctx, data).render(ab.render_opts(spp, 1, 1, 5, mode=mode))
+    px = res.film[..., 0].astype(np.float64).ravel()
+    got, se = px.mean(), px.std(ddof=1) / np.sqrt(px.size)
+    assert abs(got - want) < 4 * se + 1e-4 * want, (got, want, plain, se)
+    assert se < 0.0015 * want
