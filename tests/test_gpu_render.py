@@ -232,3 +232,16 @@ def test_ct_direct_lighting_known_answer(ctx, mode, rough):
     got, se = px.mean(), px.std(ddof=1) / np.sqrt(px.size)
     assert abs(got - want) < 4 * se + 1e-4 * want, (got, want, plain, se)
     assert se < 0.0015 * want
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_sphere_light_known_answer(ctx, mode):
+    """The sphere light's cone sampling on the device against the closed-form irradiance."""
+    import aurora_b200 as ab
+    from test_oracle import lambert_plane_under_sphere
+    data, want = lambert_plane_under_sphere()
+    res = ab.Scene(ctx, data).render(ab.render_opts(4096, 1, 1, 9, mode=mode))
+    px = res.film[..., 0].astype(np.float64).ravel()
+    got, se = px.mean(), px.std(ddof=1) / np.sqrt(px.size)
+    assert abs(got - want) < 4 * se + 1e-4 * want, (got, want, se)
+    assert se < 0.002 * want

@@ -255,6 +255,34 @@ def test_ct_direct_lighting_matches_the_analytic_integral(oracle_lib, rough):
         assert want - plain > 0.002 * plain
 
 
+def lambert_plane_under_sphere(albedo=0.6, h=1.0, radius=0.25, le=4.0, px=0.8):
+    """A Lambert plane y = 0 under a sphere light centred at (0, h, 0), seen straight down by
+    the pixels of a 16 x 16 film at fov slope 1e-4, all at P = (px, 0, 0). The sphere lies
+    wholly above P's horizon, so the irradiance at P is pi Le (R/d)^2 cos(theta) and the
+    pixel's expectation at max_depth 1 is albedo Le R^2 h / d^3 (d = |centre - P|)."""
+    from aurora_b200 import scenes
+    from aurora_b200 import _abi
+    b = scenes.SceneBuilder(16, 16, 1e-4, world_to_camera=scenes.look_at((px, 3, 0.001), (px, 0, 0)))
+    m = b.material(_abi.MAT_MATTE, diffuse=(albedo,) * 3)
+    v, f = scenes.quad((-5, 0, 5), (5, 0, 5), (5, 0, -5), (-5, 0, -5))
+    b.mesh(v, f, m, normals=np.tile([0, 1, 0], (4, 1)))
+    b.sphere_light((0.0, h, 0.0), radius, (le, le, le), 0.0)
+    d = math.hypot(px, h)
+    return b.build(), albedo * le * radius * radius * h / d ** 3
+
+
+def test_sphere_light_matches_the_analytic_irradiance(oracle_lib):
+    """Cone sampling of the sphere light (an extension of the reference) against its closed form."""
+    data, want = lambert_plane_under_sphere()
+    sc = oracle_lib.OracleScene(data, use_bvh=False)
+    spp = 16384
+    mean, m2, counts = sc.render(spp, 1, 1, seed=9, crop=(8, 8, 1, 1))
+    got = mean[0, 0, :3]
+    sigma = np.sqrt(m2[0, 0, :3] / (spp - 1)) / math.sqrt(spp)
+    assert np.all(np.abs(got - want) < 4 * sigma + 1e-4 * want), (got, want, sigma)
+    assert sigma[0] < 0.002 * want
+
+
 def test_oracle_render_is_deterministic(oracle_lib):
     from aurora_b200 import scenes
     data = scenes.box_scene(64, 64)
