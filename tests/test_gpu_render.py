@@ -245,3 +245,18 @@ def test_sphere_light_known_answer(ctx, mode):
     got, se = px.mean(), px.std(ddof=1) / np.sqrt(px.size)
     assert abs(got - want) < 4 * se + 1e-4 * want, (got, want, se)
     assert se < 0.002 * want
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_kelemen_lobe_choice_known_answer(ctx, kelemen_tables, mode):
+    """The Kelemen lobe choice on the device (its own albedo tables) against
+    A E_ct + (1 - A) E_lambert, A read from those tables at (N.V, roughness)."""
+    import aurora_b200 as ab
+    from test_oracle import kelemen_plane_under_light
+    data, want, A = kelemen_plane_under_light(kelemen_tables)
+    assert 0.05 < A < 0.95
+    res = ab.Scene(ctx, data).render(ab.render_opts(16384, 1, 1, 7, mode=mode))
+    px = res.film[..., 0].astype(np.float64).ravel()
+    got, se = px.mean(), px.std(ddof=1) / np.sqrt(px.size)
+    assert abs(got - want) < 4 * se + 1e-4 * want, (got, want, A, se)
+    assert se < 0.005 * want

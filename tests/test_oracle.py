@@ -183,40 +183,43 @@ def test_direct_lighting_matches_the_analytic_integral(oracle_lib):
     assert abs(got - want) < 4 * sigma + 1e-3 * want, (got, want, sigma)
 
 
-def ct_plane_under_light(rough, spec=0.7, h=1.0, s=0.25, le=4.0, px=0.8, eye_dist=3.0, n=1200):
-    """A Cook-Torrance (Beckmann) plane y = 0 under a downward square light centred at
-    (0, h, 0), seen by one narrow camera pixel, (8, 8) of 16 x 16 at fov slope 1e-4, that
-    looks at P = (px, 0, 0) from the mirror side of the light's centre, where the lobe
-    points. Returns the scene, the float64 expectation of that pixel at max_depth 1, and
-    the plain integral.
-
-    The plain integral is Lo = integral over the light of Le f(L, V) cos(theta) cos(theta_l)
-    / r^2 dA, with f = colour D / (4 (V.H)^2), D = exp(-tan^2 a / m^2) / (m^2 pi cos^3 a),
-    zero unless V.H, L.N and V.N exceed 1e-3 (cookTorrance.cpp:125-144). The reference's
-    estimator converges to it except in one place: its sampler sets tan a = 0 where N.H >
-    0.999 (cookTorrance.cpp:79), so inside that 2.6-degree cap the pdf it reports for a
-    sampled direction exceeds pdf() (cookTorrance.cpp:101-117) for the same direction, and
-    the two power-heuristic weights (integrator.cpp:56-98) sum to more than one there.
-    The expectation takes each strategy with its own weights: the light sample's
-    w_l = p_l^2 / (p_l^2 + p_b^2) on f, the BRDF sample's w_b = p_s^2 / (p_s^2 + p_l^2)
-    on the sampled f / pdf ratio, which is f / p_b for the Beckmann density it draws."""
+def _glossy_plane_scene(material, h, s, le, px, eye_dist):
+    """The plane y = 0 with `material` (a builder -> material index callable) under a
+    downward square light centred at (0, h, 0), seen by the 16 x 16 pixels of a camera at
+    fov slope 1e-4 that looks at P = (px, 0, 0) from the mirror side of the light's centre.
+    Returns the scene and the view direction V."""
     from aurora_b200 import scenes
-    from aurora_b200 import _abi
     P = np.array([px, 0.0, 0.0])
     mirror = np.array([px, h, 0.0]) / math.hypot(px, h)   # reflection of the light centre's direction
     eye = P + eye_dist * mirror
     b = scenes.SceneBuilder(16, 16, 1e-4, world_to_camera=scenes.look_at(tuple(eye), tuple(P)))
-    m = b.material(_abi.MAT_COOKTORRANCE, specular=(spec,) * 3, roughness=rough, reflectance=0.04)
+    m = material(b)
     v, f = scenes.quad((-5, 0, 5), (5, 0, 5), (5, 0, -5), (-5, 0, -5))
     b.mesh(v, f, m, normals=np.tile([0, 1, 0], (4, 1)))
     b.square_light(scenes.translate(0, h, 0) @ scenes.rot_x(-90.0), s, s, (le, le, le), 0.0)
-    data = b.build()
+    return b.build(), mirror
+
+
+def _light_integrals(rough, spec, V, h, s, le, px, n):
+    """Float64 quadrature over the light square of next-event estimates at P for view V.
+
+    Returns (expect, plain, lambert). plain is the Cook-Torrance integral of Le f(L, V)
+    cos(theta) cos(theta_l) / r^2 dA, with f = colour D / (4 (V.H)^2), D = exp(-tan^2 a / m^2)
+    / (m^2 pi cos^3 a), zero unless V.H, L.N and V.N exceed 1e-3 (cookTorrance.cpp:125-144).
+    The reference's estimator converges to it except in one place: its sampler sets
+    tan a = 0 where N.H > 0.999 (cookTorrance.cpp:79), so inside that 2.6-degree cap the pdf
+    it reports for a sampled direction exceeds pdf() (cookTorrance.cpp:101-117) for the same
+    direction, and the two power-heuristic weights (integrator.cpp:56-98) sum to more than
+    one there. expect takes each strategy with its own weights: the light sample's
+    w_l = p_l^2 / (p_l^2 + p_b^2) on f, the BRDF sample's w_b = p_s^2 / (p_s^2 + p_l^2) on the
+    sampled f / pdf ratio, which is f / p_b for the Beckmann density it draws. lambert is
+    the integral of Le cos(theta) cos(theta_l) / (pi r^2) dA: the Lambert estimate per unit
+    albedo (integrator.cpp:33-54, lambert.h:68-80)."""
     g = (np.arange(n) + 0.5) / n * 2 * s - s
     X, Z = np.meshgrid(g, g)
     d = np.stack([X - px, np.full_like(X, h), Z], -1)
     r = np.linalg.norm(d, axis=-1)
     L = d / r[..., None]
-    V = mirror
     Hv = L + V
     Hv /= np.linalg.norm(Hv, axis=-1, keepdims=True)
     vh, ln, vn, nh = Hv @ V, L[..., 1], V[1], Hv[..., 1]
@@ -235,9 +238,50 @@ def ct_plane_under_light(rough, spec=0.7, h=1.0, s=0.25, le=4.0, px=0.8, eye_dis
     w_b = p_s ** 2 / (p_s ** 2 + p_l ** 2)
     dA = (2 * s / n) ** 2
     geo = le * ln * cos_l / (r * r)
-    plain = float(np.sum(geo * f_eval) * dA)
-    expect = float(np.sum(geo * (f_eval * w_l + f_all * w_b)) * dA)
+    return (float(np.sum(geo * (f_eval * w_l + f_all * w_b)) * dA), float(np.sum(geo * f_eval) * dA),
+            float(np.sum(geo) * dA / math.pi))
+
+
+def ct_plane_under_light(rough, spec=0.7, h=1.0, s=0.25, le=4.0, px=0.8, eye_dist=3.0, n=1200):
+    """A Cook-Torrance (Beckmann) plane under a square light: the scene, the float64
+    expectation of every pixel at max_depth 1, and the plain integral (_light_integrals)."""
+    from aurora_b200 import _abi
+    data, V = _glossy_plane_scene(
+        lambda b: b.material(_abi.MAT_COOKTORRANCE, specular=(spec,) * 3, roughness=rough, reflectance=0.04),
+        h, s, le, px, eye_dist)
+    expect, plain, _ = _light_integrals(rough, spec, V, h, s, le, px, n)
     return data, expect, plain
+
+
+def kelemen_albedo_lookup(table, costheta, rough):
+    """KelemenMaterial::getAlbedo's bilinear lookup (kelemenMaterial.cpp:180-212) of a 64 x 32
+    table, with its second roughness column always the last one, in float64."""
+    i = min(max(int(math.floor(costheta * 63)), 0), 63)
+    ra = min(max(int(math.floor(rough * 31)), 0), 31)
+    rb = 31
+    i1 = min(i + 1, 63)
+    mixc = costheta * 63 - i
+    res_a = (1 - mixc) * table[i, ra] + mixc * table[i1, ra]
+    res_b = (1 - mixc) * table[i, rb] + mixc * table[i1, rb]
+    rmix = rough * 31 - ra
+    return (1 - rmix) * res_a + rmix * res_b
+
+
+def kelemen_plane_under_light(tables, rough=0.3, spec=0.6, diff=0.5, refl=0.04, h=1.0, s=0.25, le=4.0, px=0.8,
+                              eye_dist=3.0, n=1200):
+    """A Kelemen plane under a square light. At the camera vertex the material takes the
+    Cook-Torrance lobe (spec) with probability A = its table albedo at (N.V, roughness) and
+    otherwise the Lambert lobe (diff), without reweighting (kelemenMaterial.cpp:228-255), so
+    the pixel's expectation is A E_ct + (1 - A) diff E_lambert. Returns the scene, that
+    expectation and A."""
+    from aurora_b200 import _abi
+    data, V = _glossy_plane_scene(
+        lambda b: b.material(_abi.MAT_KELEMEN, diffuse=(diff,) * 3, specular=(spec,) * 3, roughness=rough,
+                             reflectance=refl),
+        h, s, le, px, eye_dist)
+    e_ct, _, e_lam = _light_integrals(rough, spec, V, h, s, le, px, n)
+    A = kelemen_albedo_lookup(tables[int(round(refl * 20))], float(V[1]), rough)
+    return data, A * e_ct + (1 - A) * diff * e_lam, A
 
 
 @pytest.mark.parametrize("rough", [0.15, 0.4])
@@ -253,6 +297,21 @@ def test_ct_direct_lighting_matches_the_analytic_integral(oracle_lib, rough):
     assert sigma[0] < 0.0015 * want      # the check resolves the 0.3% the cap adds at roughness 0.15
     if rough < 0.2:
         assert want - plain > 0.002 * plain
+
+
+def test_kelemen_lobe_choice_matches_the_analytic_mixture(oracle_lib):
+    """The Kelemen lobe choice against A E_ct + (1 - A) E_lambert, with a constant albedo table
+    (A = 0.35 wherever it is read) as the oracle's input."""
+    tables = np.full((21, 64, 32), 0.35, np.float32)
+    data, want, A = kelemen_plane_under_light(tables)
+    assert abs(A - 0.35) < 1e-7
+    sc = oracle_lib.OracleScene(data, tables, use_bvh=False)
+    spp = 65536
+    mean, m2, counts = sc.render(spp, 1, 1, seed=7, crop=(8, 8, 1, 1))
+    got = mean[0, 0, :3]
+    sigma = np.sqrt(m2[0, 0, :3] / (spp - 1)) / math.sqrt(spp)
+    assert np.all(np.abs(got - want) < 4 * sigma + 1e-4 * want), (got, want, sigma)
+    assert sigma[0] < 0.005 * want       # a lobe reweighted by 1/A or 1/(1-A) would move it by tens of percent
 
 
 def lambert_plane_under_sphere(albedo=0.6, h=1.0, radius=0.25, le=4.0, px=0.8):
