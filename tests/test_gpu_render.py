@@ -260,3 +260,16 @@ def test_kelemen_lobe_choice_known_answer(ctx, kelemen_tables, mode):
     got, se = px.mean(), px.std(ddof=1) / np.sqrt(px.size)
     assert abs(got - want) < 4 * se + 1e-4 * want, (got, want, A, se)
     assert se < 0.005 * want
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["plain", "wavefront"])
+def test_metal_known_answer(ctx, mode):
+    """Metal's Schlick tint and two-roughness mixture on the device against the closed form."""
+    import aurora_b200 as ab
+    from test_oracle import metal_plane_under_light
+    data, want = metal_plane_under_light()
+    res = ab.Scene(ctx, data).render(ab.render_opts(16384, 1, 1, 11, mode=mode))
+    px = res.film[..., :3].astype(np.float64).reshape(-1, 3)
+    got, se = px.mean(0), px.std(0, ddof=1) / np.sqrt(px.shape[0])
+    assert np.all(np.abs(got - want) < 4 * se + 1e-4 * want), (got, want, se)
+    assert np.all(se < 0.005 * want)

@@ -299,6 +299,37 @@ def test_ct_direct_lighting_matches_the_analytic_integral(oracle_lib, rough):
         assert want - plain > 0.002 * plain
 
 
+def metal_plane_under_light(refl=(0.9, 0.6, 0.3), gain=(1.0, 0.8, 1.2), rough_a=0.2, rough_b=0.5, mix=0.3, h=1.0,
+                            s=0.25, le=4.0, px=0.8, eye_dist=3.0, n=1200):
+    """A metal plane under a square light. MetalMaterial::getBrdf (metalMaterial.cpp:32-62)
+    takes Cook-Torrance with colour schlick(V.N, reflectance) * gain per channel, and
+    roughness A when its lobe number exceeds mix, else roughness B: the pixel's expectation
+    is (1 - mix) E_ct(A) + mix E_ct(B) at that colour. Returns the scene and the RGB
+    expectation."""
+    from aurora_b200 import _abi
+    data, V = _glossy_plane_scene(
+        lambda b: b.material(_abi.MAT_METAL, specular=refl, gain=gain, roughness=rough_a, roughness_b=rough_b,
+                             mix=mix),
+        h, s, le, px, eye_dist)
+    vn = float(V[1])
+    col = np.array([(r + (1 - vn) ** 5 * (1 - r)) * g for r, g in zip(refl, gain)])
+    e_a = _light_integrals(rough_a, 1.0, V, h, s, le, px, n)[0]
+    e_b = _light_integrals(rough_b, 1.0, V, h, s, le, px, n)[0]
+    return data, col * ((1 - mix) * e_a + mix * e_b)
+
+
+def test_metal_matches_the_analytic_mixture(oracle_lib):
+    """Metal's Schlick tint per channel and its two-roughness mixture against the closed form."""
+    data, want = metal_plane_under_light()
+    sc = oracle_lib.OracleScene(data, use_bvh=False)
+    spp = 65536
+    mean, m2, counts = sc.render(spp, 1, 1, seed=11, crop=(8, 8, 1, 1))
+    got = mean[0, 0, :3]
+    sigma = np.sqrt(m2[0, 0, :3] / (spp - 1)) / math.sqrt(spp)
+    assert np.all(np.abs(got - want) < 4 * sigma + 1e-4 * want), (got, want, sigma)
+    assert np.all(sigma < 0.005 * want)
+
+
 def test_kelemen_lobe_choice_matches_the_analytic_mixture(oracle_lib):
     """The Kelemen lobe choice against A E_ct + (1 - A) E_lambert, with a constant albedo table
     (A = 0.35 wherever it is read) as the oracle's input."""
