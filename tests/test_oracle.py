@@ -373,6 +373,28 @@ def test_sphere_light_matches_the_analytic_irradiance(oracle_lib):
     assert sigma[0] < 0.002 * want
 
 
+def test_roulette_is_unbiased_where_its_weight_stays_below_one(oracle_lib):
+    """Russian roulette (integrator.cpp:221-248) continues with probability cont, the running
+    product of lum(colour) cos / pdf, and divides the throughput by it. A Lambert bounce adds
+    2 lum(albedo) cos, so with every albedo at most 0.45 cont stays below one and the image
+    with roulette from bounce 1 has the expectation of the image without it. (Above 0.5, cont
+    can exceed one; the reference then continues and still divides by cont.)"""
+    from aurora_b200 import scenes
+    from aurora_b200 import _abi
+    data = scenes.box_scene(64, 64, wall=(0.45, 0.45, 0.45), red=(0.45, 0.05, 0.05), green=(0.1, 0.4, 0.1),
+                            box_mat=dict(type_=_abi.MAT_MATTE, diffuse=(0.4, 0.4, 0.4)))
+    sc = oracle_lib.OracleScene(data)
+    spp = 512
+    full, m2f, cf = sc.render(spp, 5, 5, 3)
+    rr, m2r, cr = sc.render(spp, 5, 1, 4)
+    assert cr[0] < 0.8 * cf[0]                      # roulette ends paths early
+    var = (m2f[..., :3] + m2r[..., :3]) / (spp - 1) / spp
+    z = (rr[..., :3] - full[..., :3]) / np.sqrt(np.maximum(var, 1e-30))
+    assert np.mean(np.abs(z) > 4) < 0.002
+    tot = (rr[..., :3].sum() - full[..., :3].sum()) / math.sqrt(var.sum())
+    assert abs(tot) < 4, tot
+
+
 def test_oracle_render_is_deterministic(oracle_lib):
     from aurora_b200 import scenes
     data = scenes.box_scene(64, 64)
