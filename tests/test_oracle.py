@@ -267,7 +267,7 @@ def kelemen_albedo_lookup(table, costheta, rough):
     return (1 - rmix) * res_a + rmix * res_b
 
 
-def kelemen_plane_under_light(tables, rough=0.3, spec=0.6, diff=0.5, refl=0.04, h=1.0, s=0.25, le=4.0, px=0.8,
+def kelemen_plane_under_light(tables, rough=0.3, spec=0.6, diff=0.5, refl=0.75, h=1.0, s=0.25, le=4.0, px=0.8,
                               eye_dist=3.0, n=1200):
     """A Kelemen plane under a square light. At the camera vertex the material takes the
     Cook-Torrance lobe (spec) with probability A = its table albedo at (N.V, roughness) and
