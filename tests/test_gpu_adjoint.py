@@ -153,3 +153,28 @@ def test_wavefront_adjoint_equals_plain_adjoint(ctx):
     assert b[2]["shadow_rays"] == a[2]["shadow_rays"]
     for x, y in ((a[0], b[0]), (a[1], b[1])):
         np.testing.assert_allclose(y, x, rtol=1e-4, atol=1e-5 * float(np.max(np.abs(x))))
+
+
+@pytest.mark.parametrize("mode", [0, 1], ids=["megakernel", "wavefront"])
+def test_albedo_gradient_known_answer(ctx, mode):
+    """Closed form: a Lambert plane under a square light at max_depth 1, seen by all 16 x 16
+    pixels at one point (fov slope 1e-4). Each pixel is albedo * E, so the gradient of the
+    film's red sum with respect to the red albedo is the sum over the albedo path by path, and
+    its expectation is 256 E (E: the quadrature of test_oracle's plane cases)."""
+    import math
+    import aurora_b200 as ab
+    from test_oracle import _plane_under_light, _light_integrals
+    albedo, h, s, le, px = 0.6, 1.0, 0.25, 4.0, 0.8
+    data = _plane_under_light(albedo, h, s, (le, le, le), px, fov=1e-4)
+    want = _light_integrals(0.3, 1.0, np.array([0.0, 1.0, 0.0]), h, s, le, px, 600)[2]
+    scene = ab.Scene(ctx, data)
+    spp, seed = 4096, 3
+    film = scene.render(ab.render_opts(spp, 1, 1, seed, mode=mode)).film
+    w = np.zeros((16, 16, 4), np.float32)
+    w[..., 0] = 1.0
+    gm, gt, _ = scene.adjoint(ab.render_opts(spp, 1, 1, seed, mode=mode), w)
+    red = film[..., 0].astype(np.float64).ravel()
+    assert abs(gm[0, 0] - red.sum() / albedo) < 1e-4 * gm[0, 0]
+    se = red.std(ddof=1) / math.sqrt(red.size) / albedo
+    assert abs(gm[0, 0] / red.size - want) < 4 * se + 1e-4 * want, (gm[0, 0] / red.size, want, se)
+    assert np.all(gm[0, 1:3] == 0.0)

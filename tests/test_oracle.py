@@ -154,10 +154,10 @@ def test_camera_and_power_heuristic(oracle_lib):
     np.testing.assert_allclose(w, [0.8, 0.5], rtol=1e-7)
 
 
-def _plane_under_light(albedo=0.6, h=1.0, s=0.25, le=(4.0, 4.0, 4.0), px=0.8):
+def _plane_under_light(albedo=0.6, h=1.0, s=0.25, le=(4.0, 4.0, 4.0), px=0.8, fov=0.01):
     from aurora_b200 import scenes
     from aurora_b200 import _abi
-    b = scenes.SceneBuilder(16, 16, 0.01, world_to_camera=scenes.look_at((px, 3, 0.001), (px, 0, 0)))
+    b = scenes.SceneBuilder(16, 16, fov, world_to_camera=scenes.look_at((px, 3, 0.001), (px, 0, 0)))
     m = b.material(_abi.MAT_MATTE, diffuse=(albedo,) * 3)
     v, f = scenes.quad((-5, 0, 5), (5, 0, 5), (5, 0, -5), (-5, 0, -5))
     b.mesh(v, f, m, normals=np.tile([0, 1, 0], (4, 1)))

@@ -165,3 +165,24 @@ def test_oracle_adjoint_light_samples_matches_fd(oracle_lib):
         fd = (_loss(oracle_lib, _perturbed_material(data, m, c, h), tables, w, spp, crop, seed, 3) -
               _loss(oracle_lib, _perturbed_material(data, m, c, -h), tables, w, spp, crop, seed, 3)) / (2 * h)
         assert abs(gm[m, c] - fd) <= 0.01 * abs(fd) + 1e-6, (m, c, gm[m, c], fd)
+
+
+def test_oracle_adjoint_albedo_matches_the_analytic_gradient(oracle_lib):
+    """Closed form: on a Lambert plane under a square light at max_depth 1 the pixel is
+    albedo * E, E = integral of Le cos(theta) cos(theta_l) / (pi r^2) over the light, so
+    d pixel / d albedo = E (the quadrature of test_oracle's plane cases)."""
+    import math
+    from test_oracle import _plane_under_light, _light_integrals
+    albedo, h, s, le, px = 0.6, 1.0, 0.25, 4.0, 0.8
+    data = _plane_under_light(albedo, h, s, (le, le, le), px)
+    want = _light_integrals(0.3, 1.0, np.array([0.0, 1.0, 0.0]), h, s, le, px, 600)[2]
+    osc = oracle_lib.OracleScene(data, use_bvh=False)
+    w = np.zeros((16, 16, 4), np.float32)
+    w[8, 8, 0] = 1.0
+    spp, seed = 4096, 3
+    gm, gt = osc.adjoint(spp, 1, 1, seed, w, crop=(8, 8, 1, 1))
+    mean, m2, _ = osc.render(spp, 1, 1, seed, crop=(8, 8, 1, 1))
+    sigma = math.sqrt(m2[0, 0, 0] / (spp - 1)) / math.sqrt(spp) / albedo
+    assert abs(gm[0, 0] - want) < 4 * sigma + 1e-3 * want, (gm[0, 0], want, sigma)
+    assert abs(gm[0, 0] - mean[0, 0, 0] / albedo) < 1e-5 * want    # the same paths, linear in the albedo
+    assert np.all(gm[0, 1:3] == 0.0)
