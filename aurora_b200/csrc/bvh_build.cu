@@ -17,6 +17,8 @@
 //   4. bottom-up SAH leaf collapse (atomic second-arrival walk)
 //   5. deterministic depth-first layout: every node derives its output slot by
 //      walking to the root, so the result is independent of thread timing.
+//   6. the 4-wide tree: an SAH-optimal grouping of the binary nodes (a bottom-up
+//      dynamic program), built level by level.
 #include "aur_bvh.cuh"
 #include "aur_shading.cuh"
 #include <cfloat>
@@ -559,35 +561,10 @@ __device__ __forceinline__ float half_area(const float lo[3], const float hi[3])
     return dx * dy + dy * dz + dz * dx;
 }
 
-// One level of the collapse: front[i] = (binary node, its 4-wide index). Interior
-// children get the next 4-wide indices and form the next level's front.
-__global__ void k_collapse4(const BvhNode* __restrict__ n2, const int2* __restrict__ front, int nfront,
+// Writes the 4-wide node at index `at` with children (lo, hi, ref)[0..n): interior children
+// get the next 4-wide indices and join the next level's front.
+__device__ void write_node4(const float (&lo)[4][3], const float (&hi)[4][3], const int (&ref)[4], int n, int at,
                             BvhNode4* __restrict__ out, int* counters, int2* __restrict__ next, int cap) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nfront) return;
-    const int2 f = front[i];
-    float lo[4][3], hi[4][3];
-    int ref[4];
-    int n = 2;
-    {
-        const BvhNode nd = n2[f.x];
-        child_of(nd, 0, lo[0], hi[0], &ref[0]);
-        child_of(nd, 1, lo[1], hi[1], &ref[1]);
-    }
-    while (n < 4) {
-        int best = -1;
-        float ba = -1.f;
-        for (int k = 0; k < n; ++k) {
-            if (ref[k] < 0) continue;
-            const float a = half_area(lo[k], hi[k]);
-            if (a > ba) { ba = a; best = k; }
-        }
-        if (best < 0) break;
-        const BvhNode c = n2[ref[best]];
-        child_of(c, 1, lo[n], hi[n], &ref[n]);
-        child_of(c, 0, lo[best], hi[best], &ref[best]);
-        ++n;
-    }
     float v[6][4];
     int r[4];
     for (int k = 0; k < 4; ++k) {
@@ -607,7 +584,7 @@ __global__ void k_collapse4(const BvhNode* __restrict__ n2, const int2* __restri
             r[k] = ref[k];
         }
     }
-    if (f.y >= cap) return;
+    if (at >= cap) return;
     BvhNode4 o;
     o.lox = make_float4(v[0][0], v[0][1], v[0][2], v[0][3]);
     o.hix = make_float4(v[1][0], v[1][1], v[1][2], v[1][3]);
@@ -617,7 +594,131 @@ __global__ void k_collapse4(const BvhNode* __restrict__ n2, const int2* __restri
     o.hiz = make_float4(v[5][0], v[5][1], v[5][2], v[5][3]);
     o.ref = make_int4(r[0], r[1], r[2], r[3]);
     o.pad = make_int4(0, 0, 0, 0);
-    out[f.y] = o;
+    out[at] = o;
+}
+
+// SAH-optimal grouping of the binary tree into 4-wide nodes: a dynamic program over the
+// binary tree, bottom up (the 8-wide form is in Ylitie, Karras and Laine, "Efficient
+// Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs", HPG 2017). The leaves are
+// fixed, so groupings differ in SAH cost only by the summed surface area of the 4-wide
+// nodes. S(x, j) is the least such sum for the subtree of binary node x when it may fill j
+// of its parent's child slots (a leaf costs nothing): S(x, 1) = A(x) + D(x, 4), and for
+// j > 1 S(x, j) = min(S(x, 1), D(x, j)), with D(x, j) = min over k in [1, j) of
+// S(left, k) + S(right, j - k). dec(x, j) is the k that reaches S(x, j), or 0 where x fills
+// one slot; dec(x, 4) is the split of x's slots when x roots a 4-wide node.
+struct Dp4 {
+    float4* S;          // S(x, 1..4)
+    uchar4* dec;        // dec(x, 1..4) (dec(x, 1) = 0)
+    int* parent;        // binary parent, -1 at the root
+    int* visit;         // arrivals so far, started at the number of leaf children
+};
+
+__global__ void k_dp4_init(const BvhNode* __restrict__ n2, int nn, Dp4 d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const BvhNode nd = n2[i];
+    const int r0 = __float_as_int(nd.d.x), r1 = __float_as_int(nd.d.y);
+    d.visit[i] = (r0 < 0) + (r1 < 0);
+    if (i == 0) d.parent[0] = -1;
+    if (r0 >= 0) d.parent[r0] = i;
+    if (r1 >= 0) d.parent[r1] = i;
+}
+
+__device__ void dp4_node(const BvhNode* __restrict__ n2, int x, Dp4 d) {
+    const BvhNode nd = n2[x];
+    float lo[2][3], hi[2][3];
+    int r[2];
+    child_of(nd, 0, lo[0], hi[0], &r[0]);
+    child_of(nd, 1, lo[1], hi[1], &r[1]);
+    float ulo[3], uhi[3];
+    for (int a = 0; a < 3; ++a) { ulo[a] = fminf(lo[0][a], lo[1][a]); uhi[a] = fmaxf(hi[0][a], hi[1][a]); }
+    float sc[2][5];
+    for (int c = 0; c < 2; ++c) {
+        sc[c][0] = 0.f;
+        if (r[c] >= 0) {
+            const float4 v = __ldcg(&d.S[r[c]]);
+            sc[c][1] = v.x; sc[c][2] = v.y; sc[c][3] = v.z; sc[c][4] = v.w;
+        } else {
+            sc[c][1] = sc[c][2] = sc[c][3] = sc[c][4] = 0.f;
+        }
+    }
+    float D[5] = {0.f, 0.f, FLT_MAX, FLT_MAX, FLT_MAX};
+    int kd[5] = {0, 0, 0, 0, 0};
+    for (int j = 2; j <= 4; ++j)
+        for (int k = 1; k < j; ++k) {
+            const float c = sc[0][k] + sc[1][j - k];
+            if (c < D[j]) { D[j] = c; kd[j] = k; }
+        }
+    const float s1 = half_area(ulo, uhi) + D[4];
+    float S[5];
+    int dec[5];
+    S[1] = s1; dec[1] = 0;
+    for (int j = 2; j <= 3; ++j) {
+        if (s1 <= D[j]) { S[j] = s1; dec[j] = 0; }
+        else { S[j] = D[j]; dec[j] = kd[j]; }
+    }
+    S[4] = D[4]; dec[4] = kd[4];   // s1 = A + D(x, 4) > D(x, 4)
+    d.S[x] = make_float4(S[1], S[2], S[3], S[4]);
+    d.dec[x] = make_uchar4(0, (unsigned char)dec[2], (unsigned char)dec[3], (unsigned char)dec[4]);
+}
+
+// Bottom-up sweep: a thread starts at each node whose children are both leaves; the last
+// child to finish carries on to the parent.
+__global__ void k_dp4(const BvhNode* __restrict__ n2, int nn, Dp4 d) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nn) return;
+    const BvhNode nd = n2[i];
+    if (__float_as_int(nd.d.x) >= 0 || __float_as_int(nd.d.y) >= 0) return;
+    int x = i;
+    while (true) {
+        dp4_node(n2, x, d);
+        __threadfence();
+        const int p = d.parent[x];
+        if (p < 0) return;
+        if (atomicAdd(&d.visit[p], 1) == 0) return;   // the sibling subtree is still running
+        __threadfence();
+        x = p;
+    }
+}
+
+__device__ __forceinline__ int dec_for(uchar4 v, int j) { return j == 2 ? v.y : j == 3 ? v.z : j == 4 ? v.w : 0; }
+
+// One level of the collapse by the program's decisions: the node's four slots are split
+// between its binary children by dec(x, 4), and a child given j > 1 slots is opened while
+// dec(child, j) says so. Slots always add up to four, so a node gets at most four children.
+__global__ void k_collapse4_dp(const BvhNode* __restrict__ n2, const uchar4* __restrict__ dec,
+                               const int2* __restrict__ front, int nfront, BvhNode4* __restrict__ out, int* counters,
+                               int2* __restrict__ next, int cap) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nfront) return;
+    const int2 f = front[i];
+    float lo[4][3], hi[4][3];
+    int ref[4], bud[4];
+    int n = 2;
+    {
+        const BvhNode nd = n2[f.x];
+        child_of(nd, 0, lo[0], hi[0], &ref[0]);
+        child_of(nd, 1, lo[1], hi[1], &ref[1]);
+        const int k = dec[f.x].w;
+        bud[0] = k;
+        bud[1] = 4 - k;
+    }
+    while (n < 4) {
+        int e = -1, dd = 0;
+        for (int q = 0; q < n && e < 0; ++q) {
+            if (ref[q] < 0 || bud[q] < 2) continue;
+            const int v = dec_for(dec[ref[q]], bud[q]);
+            if (v > 0) { e = q; dd = v; }
+        }
+        if (e < 0) break;
+        const BvhNode c = n2[ref[e]];
+        child_of(c, 1, lo[n], hi[n], &ref[n]);
+        bud[n] = bud[e] - dd;
+        child_of(c, 0, lo[e], hi[e], &ref[e]);
+        bud[e] = dd;
+        ++n;
+    }
+    write_node4(lo, hi, ref, n, f.y, out, counters, next, cap);
 }
 
 }  // namespace
@@ -638,6 +739,14 @@ cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
     CK(dalloc(&fa, cap, s));
     CK(dalloc(&fb, cap, s));
     CK(dalloc(&counters, 2, s));
+    Dp4 dp{};
+    CK(dalloc(&dp.S, cap, s));
+    CK(dalloc(&dp.dec, cap, s));
+    CK(dalloc(&dp.parent, cap, s));
+    CK(dalloc(&dp.visit, cap, s));
+    k_dp4_init<<<div_up(cap, 256), 256, 0, s>>>(b->nodes, cap, dp);
+    k_dp4<<<div_up(cap, 256), 256, 0, s>>>(b->nodes, cap, dp);
+    CK(cudaGetLastError());
     const int2 root = make_int2(0, 0);
     const int init[2] = {1, 0};
     CK(cudaMemcpyAsync(fa, &root, sizeof(int2), cudaMemcpyHostToDevice, s));
@@ -646,7 +755,7 @@ cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
     while (nfront > 0) {
         if (++levels > 64) return cudaErrorUnknown;   // the binary tree's depth is at most 63
         CK(cudaMemsetAsync(counters + 1, 0, sizeof(int), s));
-        k_collapse4<<<div_up(nfront, 256), 256, 0, s>>>(b->nodes, fa, nfront, b->nodes4, counters, fb, cap);
+        k_collapse4_dp<<<div_up(nfront, 256), 256, 0, s>>>(b->nodes, dp.dec, fa, nfront, b->nodes4, counters, fb, cap);
         CK(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
         if (hc[0] > cap || hc[1] > cap) return cudaErrorUnknown;
@@ -658,6 +767,10 @@ cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
     dfree(fa, s);
     dfree(fb, s);
     dfree(counters, s);
+    dfree(dp.S, s);
+    dfree(dp.dec, s);
+    dfree(dp.parent, s);
+    dfree(dp.visit, s);
     return cudaGetLastError();
 }
 
