@@ -248,10 +248,14 @@ __device__ __forceinline__ float half_area(float3 lo, float3 hi) {
 }
 
 constexpr int kNnBlock = 256;
+constexpr int kPlocBatch = 8;
 constexpr int kMaxRadius = 32;
 
-__global__ void __launch_bounds__(kNnBlock) k_ploc_nn(const int* clusters, int m, Tree t, int* nn, int r) {
+// The cluster count m lives on the device (dm) so that several iterations run between host
+// synchronisations; grids are sized for an upper bound of it.
+__global__ void __launch_bounds__(kNnBlock) k_ploc_nn(const int* clusters, const int* dm, Tree t, int* nn, int r) {
     __shared__ float3 s_lo[kNnBlock + 2 * kMaxRadius], s_hi[kNnBlock + 2 * kMaxRadius];
+    const int m = *dm;
     const int start = blockIdx.x * kNnBlock - r;
     const int count = kNnBlock + 2 * r;
     for (int k = threadIdx.x; k < count; k += kNnBlock) {
@@ -283,9 +287,11 @@ __global__ void __launch_bounds__(kNnBlock) k_ploc_nn(const int* clusters, int m
     nn[i] = bj;
 }
 
-__global__ void k_ploc_merge(int* clusters, int m, const int* nn, Tree t, int* node_counter, uint32_t* keep) {
+__global__ void k_ploc_merge(int* clusters, const int* dm, int bound, const int* nn, Tree t, int* node_counter,
+                             uint32_t* keep) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= m) return;
+    if (i >= bound) return;
+    if (i >= *dm) { keep[i] = 0u; return; }   // the scan runs over the bound
     const int j = nn[i];
     if (j >= 0 && nn[j] == i) {
         if (i < j) {
@@ -309,9 +315,15 @@ __global__ void k_ploc_merge(int* clusters, int m, const int* nn, Tree t, int* n
     }
 }
 
-__global__ void k_compact(const int* in, const uint32_t* keep, const uint32_t* pos, int m, int* out) {
+__global__ void k_compact(const int* in, const uint32_t* keep, const uint32_t* pos, const int* dm, int* out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < m && keep[i]) out[pos[i]] = in[i];
+    if (i < *dm && keep[i]) out[pos[i]] = in[i];
+}
+
+// The next cluster count: the kept clusters of the compaction.
+__global__ void k_ploc_count(const uint32_t* keep, const uint32_t* pos, int* dm) {
+    const int m = *dm;
+    *dm = (int)(pos[m - 1] + keep[m - 1]);
 }
 
 // ------------------------------------------------------------ SAH collapse
@@ -481,21 +493,28 @@ cudaError_t bvh_build_device(const float* verts, const uint32_t* idx, int n, con
     k_init_leaves<<<div_up(n, T), T, 0, s>>>(vals, n, plo, phi, t, ca);
     CK(cudaMemcpyAsync(counter, &n, sizeof(int), cudaMemcpyHostToDevice, s));
     const int r = opt.ploc_radius < 1 ? 1 : (opt.ploc_radius > kMaxRadius ? kMaxRadius : opt.ploc_radius);
+    // kPlocBatch iterations between host reads of the count; once one cluster is left the
+    // remaining iterations of a batch keep it as it is
     int m = n;
-    uint32_t tail[2];
+    int* dm = nullptr;
+    CK(dalloc(&dm, 1, s));
+    CK(cudaMemcpyAsync(dm, &n, sizeof(int), cudaMemcpyHostToDevice, s));
     while (m > 1) {
-        k_ploc_nn<<<div_up(m, kNnBlock), kNnBlock, 0, s>>>(ca, m, t, nn, r);
-        k_ploc_merge<<<div_up(m, T), T, 0, s>>>(ca, m, nn, t, counter, keep);
-        CK(exclusive_scan(keep, pos, m, s));
-        k_compact<<<div_up(m, T), T, 0, s>>>(ca, keep, pos, m, cb);
-        CK(cudaMemcpyAsync(&tail[0], pos + (m - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
-        CK(cudaMemcpyAsync(&tail[1], keep + (m - 1), sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+        for (int it = 0; it < kPlocBatch; ++it) {
+            k_ploc_nn<<<div_up(m, kNnBlock), kNnBlock, 0, s>>>(ca, dm, t, nn, r);
+            k_ploc_merge<<<div_up(m, T), T, 0, s>>>(ca, dm, m, nn, t, counter, keep);
+            CK(exclusive_scan(keep, pos, m, s));
+            k_compact<<<div_up(m, T), T, 0, s>>>(ca, keep, pos, dm, cb);
+            k_ploc_count<<<1, 1, 0, s>>>(keep, pos, dm);
+            std::swap(ca, cb);
+        }
+        int m2 = 0;
+        CK(cudaMemcpyAsync(&m2, dm, sizeof(int), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        const int m2 = (int)(tail[0] + tail[1]);
-        if (m2 >= m) return cudaErrorUnknown;   // no progress: impossible with the strict pair order
+        if (m2 < 1 || (m2 > 1 && m2 >= m)) return cudaErrorUnknown;   // no progress: impossible with the strict pair order
         m = m2;
-        std::swap(ca, cb);
     }
+    dfree(dm, s);
     int root = 0;
     CK(cudaMemcpyAsync(&root, ca, sizeof(int), cudaMemcpyDeviceToHost, s));
 
@@ -681,16 +700,25 @@ __global__ void k_dp4(const BvhNode* __restrict__ n2, int nn, Dp4 d) {
     }
 }
 
+// Between two levels: the next front becomes the current one (c[2]) and a non-empty level
+// is counted (c[3]).
+constexpr int kCollapseBatch = 8;
+__global__ void k_collapse_next(int* c) {
+    if (c[2] > 0) ++c[3];
+    c[2] = c[1];
+    c[1] = 0;
+}
+
 __device__ __forceinline__ int dec_for(uchar4 v, int j) { return j == 2 ? v.y : j == 3 ? v.z : j == 4 ? v.w : 0; }
 
 // One level of the collapse by the program's decisions: the node's four slots are split
 // between its binary children by dec(x, 4), and a child given j > 1 slots is opened while
 // dec(child, j) says so. Slots always add up to four, so a node gets at most four children.
 __global__ void k_collapse4_dp(const BvhNode* __restrict__ n2, const uchar4* __restrict__ dec,
-                               const int2* __restrict__ front, int nfront, BvhNode4* __restrict__ out, int* counters,
-                               int2* __restrict__ next, int cap) {
+                               const int2* __restrict__ front, const int* nfront, BvhNode4* __restrict__ out,
+                               int* counters, int2* __restrict__ next, int cap) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nfront) return;
+    if (i >= *nfront) return;
     const int2 f = front[i];
     float lo[4][3], hi[4][3];
     int ref[4], bud[4];
@@ -738,7 +766,7 @@ cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
     }
     CK(dalloc(&fa, cap, s));
     CK(dalloc(&fb, cap, s));
-    CK(dalloc(&counters, 2, s));
+    CK(dalloc(&counters, 4, s));
     Dp4 dp{};
     CK(dalloc(&dp.S, cap, s));
     CK(dalloc(&dp.dec, cap, s));
@@ -748,22 +776,31 @@ cudaError_t bvh_collapse4(DeviceBvh* b, cudaStream_t s) {
     k_dp4<<<div_up(cap, 256), 256, 0, s>>>(b->nodes, cap, dp);
     CK(cudaGetLastError());
     const int2 root = make_int2(0, 0);
-    const int init[2] = {1, 0};
+    // counters: next 4-wide index, next front's size, this front's size, non-empty levels.
+    // kCollapseBatch levels run between host reads; the grid covers an upper bound of the
+    // front (at most four times the previous one, and at most cap)
+    const int init[4] = {1, 0, 1, 0};
     CK(cudaMemcpyAsync(fa, &root, sizeof(int2), cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(counters, init, sizeof(init), cudaMemcpyHostToDevice, s));
-    int nfront = 1, levels = 0, hc[2] = {1, 0};
-    while (nfront > 0) {
-        if (++levels > 64) return cudaErrorUnknown;   // the binary tree's depth is at most 63
-        CK(cudaMemsetAsync(counters + 1, 0, sizeof(int), s));
-        k_collapse4_dp<<<div_up(nfront, 256), 256, 0, s>>>(b->nodes, dp.dec, fa, nfront, b->nodes4, counters, fb, cap);
+    int bound = 1, launched = 0, hc[4] = {1, 0, 1, 0};
+    while (true) {
+        for (int it = 0; it < kCollapseBatch; ++it) {
+            k_collapse4_dp<<<div_up(bound, 256), 256, 0, s>>>(b->nodes, dp.dec, fa, counters + 2, b->nodes4, counters,
+                                                              fb, cap);
+            k_collapse_next<<<1, 1, 0, s>>>(counters);
+            std::swap(fa, fb);
+            bound = (int)std::min<long long>(cap, 4ll * bound);
+        }
+        launched += kCollapseBatch;
         CK(cudaMemcpyAsync(hc, counters, sizeof(hc), cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
-        if (hc[0] > cap || hc[1] > cap) return cudaErrorUnknown;
-        nfront = hc[1];
-        std::swap(fa, fb);
+        if (hc[0] > cap || hc[2] > cap) return cudaErrorUnknown;
+        if (hc[2] == 0) break;
+        if (launched > 64) return cudaErrorUnknown;   // the binary tree's depth is at most 63
+        bound = hc[2];
     }
     b->num_nodes4 = hc[0];
-    b->depth4 = levels;
+    b->depth4 = hc[3];
     dfree(fa, s);
     dfree(fb, s);
     dfree(counters, s);
