@@ -81,6 +81,7 @@ struct WfPool {
     uint32_t* state;            // PS_* in the low bits, PS_PENDING when next-event rays are in flight
     uint32_t* sh_vis;           // bit k: next-event ray k of the slot is unoccluded
     uint32_t* rec_cur;          // record mode: record index of the vertex whose next-event rays are in flight
+    uint8_t* bucket;            // material bucket of the slot's last hit (written by the sorting extend)
     uint32_t *q_ext0, *q_ext1, *q_sort, *q_shadow;
     uint32_t* ctr;
     unsigned long long* rays;   // [0] closest-hit rays, [1] shadow rays
@@ -334,7 +335,10 @@ __global__ void __launch_bounds__(256, AUR_TRAV_MINB) k_extend(WfPool w, int in_
         int bucket = -1;
         if (done) {
             w.hit(slot) = make_float4(ts.tbest, ts.bu, ts.bv, __int_as_float(ts.best));
-            if (kSort) bucket = bucket_of(S->sc.sh, ts.best);
+            if (kSort) {
+                bucket = bucket_of(S->sc.sh, ts.best);
+                w.bucket[slot] = (uint8_t)bucket;   // the scatter reads it instead of the hit's material
+            }
             has = false;
         }
         if (kSort) {   // per-bucket counts, one shared atomic per (warp, bucket)
@@ -372,8 +376,7 @@ __global__ void k_sort_scatter(WfPool w, int in_q) {
         uint32_t slot = 0, local = 0;
         if (k < n) {
             slot = qin[k];
-            const int prim = __float_as_int(w.hit(slot).w);
-            bucket = bucket_of(w.scenes[w.id(slot).x].sc.sh, prim);
+            bucket = w.bucket[slot];
         }
         const uint32_t active = __ballot_sync(0xffffffffu, bucket >= 0);
         if (bucket >= 0) {
@@ -738,7 +741,7 @@ struct WfRun {
         cfg = c;
         stream = s;
         const size_t P = c.pool;
-        const size_t bytes = P * (12 * sizeof(float4) + 8 * sizeof(uint32_t)) + 20 * 256 +
+        const size_t bytes = P * (12 * sizeof(float4) + 8 * sizeof(uint32_t) + 1) + 21 * 256 +
                              kCounters * sizeof(uint32_t) + 2 * sizeof(unsigned long long);
         cudaError_t e = cudaMalloc(&mem, bytes);
         if (e != cudaSuccess) return e;
@@ -753,6 +756,7 @@ struct WfRun {
         w.q_shadow = (uint32_t*)take(2 * P * 4);   // up to two next-event rays per slot
         w.sh_vis = (uint32_t*)take(P * 4);
         w.rec_cur = (uint32_t*)take(P * 4);
+        w.bucket = (uint8_t*)take(P);
         w.ctr = (uint32_t*)take(kCounters * 4);
         w.rays = (unsigned long long*)take(2 * sizeof(unsigned long long));
         if ((size_t)(p - (char*)mem) > bytes) return cudaErrorMemoryAllocation;
