@@ -786,7 +786,9 @@ struct WfRun {
         grid_shade_r = persist(c.record ? (const void*)k_shade<true, SHADE_REST> : (const void*)k_shade<false, SHADE_REST>, 0);
         grid_shadow = persist(c.wide ? (const void*)k_shadow<true> : (const void*)k_shadow<false>, stack_smem);
         grid_sort = persist((const void*)k_sort_scatter, 0);
-        grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 16);
+        // 64 blocks per SM (about 10 resident waves of the 40-register kernel): 14.8 ms per
+        // 1080p frame against 15.3 at 16 and 16.5 at exactly the resident 6
+        grid_regen = (int)std::min<size_t>((P + c.block - 1) / c.block, (size_t)sms * 64);
         return cudaSuccess;
     }
 
