@@ -178,3 +178,31 @@ def test_albedo_gradient_known_answer(ctx, mode):
     se = red.std(ddof=1) / math.sqrt(red.size) / albedo
     assert abs(gm[0, 0] / red.size - want) < 4 * se + 1e-4 * want, (gm[0, 0] / red.size, want, se)
     assert np.all(gm[0, 1:3] == 0.0)
+
+
+def test_adjoint_sharded_one_rank_equals_adjoint(ctx):
+    """aurora_b200.shard.adjoint_sharded in a one-rank gloo group (its combine is then the
+    identity) gives the device adjoint of the whole sample range."""
+    import datetime
+    import socket
+    import torch.distributed as dist
+    import aurora_b200 as ab
+    from aurora_b200 import scenes
+    from aurora_b200.shard import adjoint_sharded
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        data = scenes.texture_scene(64, 64)
+        scene = ab.Scene(ctx, data)
+        w = np.random.default_rng(4).normal(size=(64, 64, 4)).astype(np.float32)
+        opts = ab.render_opts(16, 6, 6, 2, mode=1)
+        gm, gt = adjoint_sharded(scene, opts, w)
+        gm1, gt1, _ = scene.adjoint(ab.render_opts(16, 6, 6, 2, mode=1), w)
+        np.testing.assert_allclose(gm, gm1, rtol=1e-6, atol=1e-7)
+        np.testing.assert_allclose(gt, gt1, rtol=1e-6, atol=1e-7)
+        assert np.any(gm != 0)
+    finally:
+        dist.destroy_process_group()

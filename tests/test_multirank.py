@@ -66,3 +66,43 @@ def test_sharded_render_equals_single_render(tmp_path, oracle_lib, world, spp):
     osc = oracle_lib.OracleScene(data, np.zeros((21, 64, 32), np.float32))
     whole, _, _ = osc.render(spp, 5, 5, 1, threads=1, want_m2=False)
     np.testing.assert_allclose(combined, whole, rtol=1e-6, atol=1e-6)
+
+
+def _adjoint_worker(rank, world, port, spp, result_path):
+    import datetime
+    import torch.distributed as dist
+    from aurora_b200 import scenes
+    from aurora_b200.shard import combine_gradients, sample_range
+    from oracle import oracle
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    try:
+        data = scenes.texture_scene(24, 24)
+        osc = oracle.OracleScene(data, np.zeros((21, 64, 32), np.float32))
+        w = np.random.default_rng(3).normal(size=(24, 24, 4)).astype(np.float32)
+        first, count = sample_range(rank, world, spp)
+        gm, gt = osc.adjoint(count, 6, 6, 2, w, sample_offset=first, threads=1)
+        combine_gradients((gm, gt), count, spp)
+        if rank == 0:
+            np.save(result_path, np.concatenate([gm.ravel(), gt.ravel()]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,spp", [(2, 6), (3, 7)])
+def test_sharded_adjoint_equals_single_adjoint(tmp_path, oracle_lib, world, spp):
+    """Each rank's adjoint over its sample range, combined by combine_gradients (one sum
+    all-reduce of the count-weighted gradients), equals the adjoint over all samples."""
+    import torch.multiprocessing as mp
+    from aurora_b200 import scenes
+    path = str(tmp_path / "grad.npy")
+    mp.start_processes(_adjoint_worker, args=(world, _free_port(), spp, path), nprocs=world, join=True,
+                       start_method="spawn")
+    combined = np.load(path)
+    data = scenes.texture_scene(24, 24)
+    osc = oracle_lib.OracleScene(data, np.zeros((21, 64, 32), np.float32))
+    w = np.random.default_rng(3).normal(size=(24, 24, 4)).astype(np.float32)
+    gm, gt = osc.adjoint(spp, 6, 6, 2, w, threads=1)
+    whole = np.concatenate([gm.ravel(), gt.ravel()])
+    assert np.any(whole != 0)
+    np.testing.assert_allclose(combined, whole, rtol=1e-9, atol=1e-12)
